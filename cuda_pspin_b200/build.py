@@ -1,0 +1,116 @@
+"""In-tree build of the engine (libpspin.so), its drivers and the oracle.
+
+    python -m cuda_pspin_b200.build          # everything
+    python -m cuda_pspin_b200.build --lib    # libpspin.so only
+
+Outputs stay inside the repository (cuda_pspin_b200/lib, cuda_pspin_b200/bin,
+oracle/liboracle.so) so that they travel with the source tree.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB_DIR = os.path.join(HERE, "lib")
+BIN_DIR = os.path.join(HERE, "bin")
+CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA, "bin", "nvcc")
+HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "layout.cpp"]
+DRIVERS = {
+    "pspin_pt": ["drivers/pt_main.cpp"],
+    "pspin_pt_sparse": ["drivers/pt_sparse_main.cpp"],
+    "pspin_mc": ["drivers/mc_main.cpp"],
+}
+
+
+def _run(cmd: list[str]) -> None:
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def _newer(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build_lib(force: bool = False) -> str:
+    os.makedirs(LIB_DIR, exist_ok=True)
+    out = os.path.join(LIB_DIR, "libpspin.so")
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp", ".h", ".cuh"))]
+    deps.append(os.path.join(ROOT, "include", "pspin.h"))
+    if not force and not _newer(out, deps):
+        return out
+    srcs = [os.path.join(CSRC, f) for f in LIB_SOURCES]
+    cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-ccbin", HOST_CXX,
+           "-Xcompiler", "-fPIC,-fopenmp,-O3", "-Xptxas", "-v" if os.environ.get("PSPIN_PTXAS_V") else "-O3",
+           "-shared", "-o", out, *srcs, "-lcurand", "-lgomp",
+           "-Xlinker", f"-rpath,{CUDA}/lib64"]
+    _run(cmd)
+    return out
+
+
+def build_drivers(force: bool = False) -> None:
+    os.makedirs(BIN_DIR, exist_ok=True)
+    lib = os.path.join(LIB_DIR, "libpspin.so")
+    common = [os.path.join(CSRC, "drivers", "common.cpp")]
+    for name, srcs in DRIVERS.items():
+        paths = [os.path.join(CSRC, s) for s in srcs]
+        if not all(os.path.exists(p) for p in paths):
+            continue
+        out = os.path.join(BIN_DIR, name)
+        deps = paths + common + [lib, os.path.join(CSRC, "drivers", "common.h")]
+        if not force and not _newer(out, deps):
+            continue
+        _run([HOST_CXX, "-O2", "-std=c++17", "-Wall", f"-I{ROOT}/include", f"-I{CSRC}/drivers",
+              *paths, *common, "-o", out, f"-L{LIB_DIR}", "-lpspin",
+              f"-Wl,-rpath,$ORIGIN/../lib", f"-Wl,-rpath,{CUDA}/lib64"])
+
+
+def build_oracle(force: bool = False) -> None:
+    odir = os.path.join(ROOT, "oracle")
+    out = os.path.join(odir, "liboracle.so")
+    deps = [os.path.join(odir, "oracle.c"), os.path.join(odir, "oracle.h")]
+    if not force and not _newer(out, deps):
+        return
+    _run(["make", "-C", odir, "liboracle.so"])
+
+
+def build_ref() -> None:
+    """Reference rebuild for sm_100a under oracle/_ref (only where the
+    reference sources are present)."""
+    if not os.path.isdir("/root/reference/src"):
+        return
+    if shutil.which("make") is None:
+        return
+    _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"])
+
+
+def main(argv: list[str] | None = None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--lib", action="store_true")
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--no-ref", action="store_true")
+    a = ap.parse_args(argv)
+    build_lib(a.force)
+    if a.lib:
+        return 0
+    build_drivers(a.force)
+    build_oracle(a.force)
+    if not a.no_ref:
+        build_ref()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,1301 @@
+// abi.cu -- the extern "C" boundary (include/pspin.h) and host orchestration.
+//
+// mc_init / mc_sparse_init (mc.cu:411-562, mc_sparse.cu:390-604) become
+// pspin_create_batch: the same cuRAND host-API calls with the same seeds
+// produce the same FP64 disorder and initial amplitudes; FMC masks and
+// survivor counts run on the device; the sweep layout is built on the host.
+#include <cuda_runtime.h>
+#include <curand.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/pspin.h"
+#include "internal.h"
+#include "layout.h"
+#include "rng.cuh"
+
+namespace pspin {
+cudaError_t dev_fmc_mask(uint8_t* mask, const double* omega, int N, double gamma, cudaStream_t st);
+cudaError_t dev_survivor_counts(unsigned long long* counts, const double* omega, int N, double gamma, cudaStream_t st);
+cudaError_t dev_popcount(const uint8_t* mask, int64_t n, unsigned long long* out, cudaStream_t st);
+cudaError_t dev_g4_real(const double* normals, double* g4, int64_t n, double sigma, double mean, cudaStream_t st);
+cudaError_t dev_gather_real(const double* normals, const int64_t* qs, int n, double* out, cudaStream_t st);
+cudaError_t dev_roundtrip(int N, int64_t nq, unsigned long long* fails, cudaStream_t st);
+}  // namespace pspin
+
+using namespace pspin;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                     \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return fail(PSPIN_ERR_CUDA, "CUDA error at %s:%d: %s", __FILE__, __LINE__,             \
+                        cudaGetErrorString(e_));                                                     \
+    } while (0)
+
+#define CKR(call)                                                                                    \
+    do {                                                                                             \
+        curandStatus_t e_ = (call);                                                                  \
+        if (e_ != CURAND_STATUS_SUCCESS)                                                             \
+            return fail(PSPIN_ERR_CURAND, "cuRAND error at %s:%d: %d", __FILE__, __LINE__, (int)e_); \
+    } while (0)
+
+#define TRY(call)                      \
+    do {                               \
+        int rc_ = (call);              \
+        if (rc_ != PSPIN_OK) return rc_; \
+    } while (0)
+
+template <class T>
+static int dalloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) return PSPIN_OK;
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(PSPIN_ERR_ALLOC, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+    }
+    return PSPIN_OK;
+}
+
+// ------------------------------------------------------------------ state
+struct SampleHost {
+    pspin_config cfg;
+    int N = 0, R = 0;
+    std::vector<double> omega;
+    std::vector<double> g2re;        // N*N (real parts; imag is 0)
+    int64_t n_pairs_active = 0, n_quart_active = 0;
+    int h2_active = 0;
+    std::vector<int32_t> sq;         // sparse: [n][5]
+    std::vector<double> sqg;
+    int64_t site_entries = 0;
+    int64_t g4_off = -1;             // dense: into d_g4re / d_mask
+    int64_t nq_dense = 0;
+};
+
+struct pspin_state {
+    int variant = 0;
+    int S = 0;
+    pspin_options opt{};
+    std::vector<SampleHost> hs;
+    std::vector<SampleDev> sd;
+    std::vector<Unit> units;
+    int R_tot = 0, max_N = 0, warps = 8;
+    int64_t spin_total = 0;
+    cudaStream_t st = nullptr;
+    int device = 0;
+
+    SampleDev* d_samples = nullptr;
+    Unit* d_units = nullptr;
+    float2* d_spins = nullptr;
+    double *d_E = nullptr, *d_beta = nullptr, *d_target = nullptr, *d_drift = nullptr, *d_e2 = nullptr,
+           *d_e4 = nullptr;
+    long long *d_acc = nullptr, *d_prop = nullptr;
+    uint64_t* d_key = nullptr;
+    int2* d_entries = nullptr;
+    int64_t* d_chunk_start = nullptr;
+    int* d_site_chunks = nullptr;
+    Q64* d_q64 = nullptr;
+    double* d_g2 = nullptr;
+    double* d_g4re = nullptr;
+    uint8_t* d_mask = nullptr;
+    long long* d_sweep_counter = nullptr;
+    int* d_status = nullptr;
+
+    // parallel tempering
+    int pt_NT = 0, pt_nrep = 0, pt_freq = 0;
+    double* d_beta_sched = nullptr;
+    int* d_perm = nullptr;
+    unsigned long long* d_drand = nullptr;
+    long long *d_ex_acc = nullptr, *d_ex_prop = nullptr;
+
+    // trace
+    pspin_move_record* d_trace = nullptr;
+    long long trace_sweep0 = 0;
+
+    long long sweeps_done = 0;
+    long long since_resync = 0;
+
+    // measurement
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+    size_t ev_used = 0;
+    long long sweep_launches = 0, kernel_launches = 0;
+};
+
+static void free_state(pspin_state* s) {
+    if (!s) return;
+    void* ptrs[] = {s->d_samples, s->d_units, s->d_spins, s->d_E, s->d_beta, s->d_target, s->d_drift,
+                    s->d_e2, s->d_e4, s->d_acc, s->d_prop, s->d_key, s->d_entries, s->d_chunk_start, s->d_site_chunks,
+                    s->d_q64, s->d_g2, s->d_g4re, s->d_mask, s->d_sweep_counter, s->d_status,
+                    s->d_beta_sched, s->d_perm, s->d_drand, s->d_ex_acc, s->d_ex_prop, s->d_trace};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (auto& e : s->ev_pool) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+}
+
+// ------------------------------------------------------------------ config
+extern "C" void pspin_default_config(pspin_config* c) {
+    // config.h:28-46
+    std::memset(c, 0, sizeof(*c));
+    c->N = 64;
+    c->nrep = 1;
+    c->T = 1.0;
+    c->J = 2.0;
+    c->J0 = 0.0;
+    c->alpha = 0.5;
+    c->alpha0 = 0.5;
+    c->mc_iterations = 10000;
+    c->seed = 42;
+    c->save_freq = 100;
+    c->verbose = 0;
+    c->label = -1;
+    c->dev = -1;
+    c->fmc_mode = 0;
+    c->gamma = 0.0;
+}
+
+extern "C" int pspin_parse_args(int argc, char** argv, pspin_config* cfg) {
+    // config.cu:6-70, with exit(1) replaced by PSPIN_ERR_ARG
+    if (!cfg) return fail(PSPIN_ERR_ARG, "null config");
+    pspin_default_config(cfg);
+    for (int i = 1; i < argc; i++) {
+        const char* a = argv[i];
+        bool has = i + 1 < argc;
+        if (!strcmp(a, "-N") && has) cfg->N = atoi(argv[++i]);
+        else if (!strcmp(a, "-nrep") && has) cfg->nrep = atoi(argv[++i]);
+        else if (!strcmp(a, "-T") && has) cfg->T = atof(argv[++i]);
+        else if (!strcmp(a, "-J") && has) cfg->J = atof(argv[++i]);
+        else if (!strcmp(a, "-J0") && has) cfg->J0 = atof(argv[++i]);
+        else if (!strcmp(a, "-alpha") && has) cfg->alpha = atof(argv[++i]);
+        else if (!strcmp(a, "-alpha0") && has) cfg->alpha0 = atof(argv[++i]);
+        else if (!strcmp(a, "-iter") && has) cfg->mc_iterations = atoi(argv[++i]);
+        else if (!strcmp(a, "-seed") && has) cfg->seed = strtoull(argv[++i], nullptr, 10);
+        else if (!strcmp(a, "-save_freq") && has) cfg->save_freq = atoi(argv[++i]);
+        else if (!strcmp(a, "-label") && has) cfg->label = atoi(argv[++i]);
+        else if (!strcmp(a, "-dev") && has) cfg->dev = atoi(argv[++i]);
+        else if (!strcmp(a, "-fmc") && has) cfg->fmc_mode = atoi(argv[++i]);
+        else if (!strcmp(a, "-gamma") && has) cfg->gamma = atof(argv[++i]);
+        else if (!strcmp(a, "-verbose")) {
+            if (i + 1 < argc && argv[i + 1][0] >= '0' && argv[i + 1][0] <= '9') cfg->verbose = atoi(argv[++i]);
+            else cfg->verbose = 1;
+        } else {
+            return fail(PSPIN_ERR_ARG,
+                        "Unknown argument: %s\nUsage: %s [-N n] [-nrep n] [-T temp] [-J coupling] [-J0 mean] "
+                        "[-alpha a] [-alpha0 a0] [-iter n] [-seed s] [-save_freq k] [-label l] [-dev d] "
+                        "[-fmc 0|1|2] [-gamma g] [-verbose [0|1|2]]",
+                        a, argc > 0 ? argv[0] : "pspin");
+        }
+    }
+    if (cfg->N < 4) return fail(PSPIN_ERR_ARG, "Error: N must be >= 4 for 4-body interactions.");
+    if (cfg->fmc_mode > 0 && cfg->gamma <= 0.0) {
+        if (cfg->fmc_mode == 1) cfg->gamma = 0.0;
+        else if (cfg->fmc_mode == 2) cfg->gamma = 1.0 / (2.0 * (cfg->N - 1));
+    }
+    return PSPIN_OK;
+}
+
+// ------------------------------------------------------------------ set-up helpers
+static inline int64_t C4(int64_t n) { return n * (n - 1) * (n - 2) * (n - 3) / 24; }
+static inline int64_t C3(int64_t n) { return n * (n - 1) * (n - 2) / 6; }
+static inline int64_t C2(int64_t n) { return n * (n - 1) / 2; }
+
+struct Curand {
+    curandGenerator_t g = nullptr;
+    ~Curand() {
+        if (g) curandDestroyGenerator(g);
+    }
+};
+
+// curandGenerateNormalDouble(PHILOX4_32_10, seed) into device memory; a fresh
+// generator per call, as in disorder.cu:61-68 and spins.cu:75-82
+static int curand_normals(uint64_t seed, size_t count, double* d_out, cudaStream_t st) {
+    Curand c;
+    CKR(curandCreateGenerator(&c.g, CURAND_RNG_PSEUDO_PHILOX4_32_10));
+    CKR(curandSetStream(c.g, st));
+    CKR(curandSetPseudoRandomGeneratorSeed(c.g, seed));
+    CKR(curandGenerateNormalDouble(c.g, d_out, count, 0.0, 1.0));
+    return PSPIN_OK;
+}
+
+static void omega_of(const pspin_config& c, std::vector<double>& w) {
+    // mc.cu:449-460
+    w.resize(c.N);
+    if (c.fmc_mode == 1) {
+        for (int i = 0; i < c.N; i++) w[i] = (double)i;
+    } else {
+        uint64_t st = c.seed + 3000;
+        for (int i = 0; i < c.N; i++) {
+            uint64_t z = splitmix64(st);
+            w[i] = (double)(z >> 11) / (double)(1ULL << 53);
+        }
+        std::sort(w.begin(), w.end());
+    }
+}
+
+// g2 generation, FMC, survivor count, rescale, mean shift
+// (mc.cu:443-444, 465-478, 491-498; disorder.cu:57-91, 130-143)
+static int setup_g2(SampleHost& h, cudaStream_t st) {
+    const pspin_config& c = h.cfg;
+    const int N = c.N;
+    const double J2 = (1.0 - c.alpha) * c.J, J20 = (1.0 - c.alpha0) * c.J0;
+    h.g2re.assign((size_t)N * N, 0.0);
+    if (c.fmc_mode != 1) {
+        double* d = nullptr;
+        TRY(dalloc(&d, 2 * (size_t)N * N));
+        int rc = curand_normals(c.seed + 1000, 2 * (size_t)N * N, d, st);
+        std::vector<double> nrm(2 * (size_t)N * N);
+        if (rc == PSPIN_OK) {
+            cudaError_t e = cudaMemcpyAsync(nrm.data(), d, nrm.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) rc = fail(PSPIN_ERR_CUDA, "g2 copy: %s", cudaGetErrorString(e));
+        }
+        cudaFree(d);
+        if (rc != PSPIN_OK) return rc;
+        // imag dropped, lower triangle copied from the upper one, diagonal kept
+        for (int i = 0; i < N; i++)
+            for (int j = 0; j < N; j++) {
+                const size_t src = (i > j) ? (size_t)j * N + i : (size_t)i * N + j;
+                h.g2re[(size_t)i * N + j] = nrm[2 * src];
+            }
+    }
+    if (c.fmc_mode > 0) {
+        omega_of(c, h.omega);
+        if (c.fmc_mode == 1) {
+            h.n_pairs_active = 0;
+        } else {
+            for (int i = 0; i < N; i++)
+                for (int j = i + 1; j < N; j++)
+                    if (std::fabs(h.omega[i] - h.omega[j]) > c.gamma) {
+                        h.g2re[(size_t)i * N + j] = 0.0;
+                        h.g2re[(size_t)j * N + i] = 0.0;
+                    }
+            int64_t n = 0;
+            for (int i = 0; i < N; i++)
+                for (int j = i; j < N; j++)
+                    if (h.g2re[(size_t)i * N + j] != 0.0) n++;
+            h.n_pairs_active = n;
+        }
+    } else {
+        h.omega.clear();
+        h.n_pairs_active = (int64_t)N * (N + 1) / 2;
+    }
+    if (h.n_pairs_active > 0) {
+        const double sigma = J2 * std::sqrt((double)N / (double)h.n_pairs_active);
+        for (double& v : h.g2re) v *= sigma;
+    }
+    if (J20 != 0.0 && h.n_pairs_active > 0) {
+        const double mean = J20 * (double)N / (double)h.n_pairs_active;
+        for (double& v : h.g2re)
+            if (v != 0.0) v += mean;
+    }
+    h.h2_active = h.n_pairs_active > 0 ? 1 : 0;
+    return PSPIN_OK;
+}
+
+// spins.cu:27-69 (sphere) / spins_sparse.cu:28-61 (cube), on the host in
+// FP64.  Returns the constraint value of the normalised amplitudes.
+static double normalize_host(double* sp, int N, int cube, int exact) {
+    if (!cube) {
+        double norm = 0.0;
+        if (exact || N > 1024) {
+            for (int i = 0; i < N; i++) norm += sp[2 * i] * sp[2 * i] + sp[2 * i + 1] * sp[2 * i + 1];
+        } else {
+            std::vector<double> s(N);
+            for (int t = 0; t < N; t++) s[t] = sp[2 * t] * sp[2 * t] + sp[2 * t + 1] * sp[2 * t + 1];
+            for (int w = N / 2; w > 0; w >>= 1)
+                for (int t = 0; t < w; t++) s[t] += s[t + w];
+            norm = s[0];
+        }
+        const double scale = std::sqrt((double)N / norm);
+        for (int i = 0; i < 2 * N; i++) sp[i] *= scale;
+        double r = 0.0;
+        for (int i = 0; i < N; i++) r += sp[2 * i] * sp[2 * i] + sp[2 * i + 1] * sp[2 * i + 1];
+        return r;
+    }
+    int bd = (N < 1024) ? ((N + 31) / 32 * 32) : 1024;
+    if (bd < 32) bd = 32;
+    double sum = 0.0;
+    if (exact) {
+        for (int i = 0; i < N; i++) {
+            const double r2 = sp[2 * i] * sp[2 * i] + sp[2 * i + 1] * sp[2 * i + 1];
+            sum += r2 * r2;
+        }
+    } else {
+        std::vector<double> s(bd, 0.0);
+        for (int t = 0; t < bd && t < N; t++) {
+            const double r2 = sp[2 * t] * sp[2 * t] + sp[2 * t + 1] * sp[2 * t + 1];
+            s[t] = r2 * r2;
+        }
+        for (int w = bd / 2; w > 0; w >>= 1)
+            for (int t = 0; t < w; t++) s[t] += s[t + w];
+        sum = s[0];
+    }
+    const double scale = std::pow((double)N / sum, 0.25);
+    const int lim = exact ? N : std::min(N, bd);
+    for (int i = 0; i < 2 * lim; i++) sp[i] *= scale;
+    double r = 0.0;
+    for (int i = 0; i < N; i++) {
+        const double r2 = sp[2 * i] * sp[2 * i] + sp[2 * i + 1] * sp[2 * i + 1];
+        r += r2 * r2;
+    }
+    return r;
+}
+
+// The idx-th survivor (q*3+ch, in ascending order) given survivor counts of
+// the (l,k) blocks and their prefix sums.
+struct SurvivorIndex {
+    int N = 0;
+    int fmc = 0;
+    double gamma = 0.0;
+    const double* w = nullptr;
+    std::vector<int> bl, bk;          // non-empty blocks in q order
+    std::vector<int64_t> pre;         // prefix (size blocks+1)
+    int64_t total = 0;
+
+    int64_t at(int64_t idx) const {
+        if (fmc == 0) return idx * 3;          // every quartet, channel 0
+        size_t b = std::upper_bound(pre.begin(), pre.end(), idx) - pre.begin() - 1;
+        const int l = bl[b], k = bk[b];
+        int64_t left = idx - pre[b];
+        const int64_t base = C4(l) + C3(k);
+        int64_t p = 0;
+        for (int j = 1; j < k; j++)
+            for (int i = 0; i < j; i++, p++) {
+                const double wi = w[i], wj = w[j], wk = w[k], wl = w[l];
+                uint8_t m = 0;
+                if (std::fabs(wi + wj - wk - wl) <= gamma) m = 1;
+                else if (std::fabs(wi + wl - wj - wk) <= gamma) m = 2;
+                else if (std::fabs(wi + wk - wj - wl) <= gamma) m = 4;
+                for (int ch = 0; ch < 3; ch++)
+                    if (m & (1 << ch)) {
+                        if (left == 0) return (base + p) * 3 + ch;
+                        left--;
+                    }
+            }
+        return -1;
+    }
+};
+
+static void decode_q(int64_t q, int& i, int& j, int& k, int& l) {
+    // mc_sparse.cu:320-335
+    int ll = 3;
+    while (C4(ll) <= q) ll++;
+    ll--;
+    int64_t rem = q - C4(ll);
+    int kk = 2;
+    while (C3(kk) <= rem) kk++;
+    kk--;
+    rem -= C3(kk);
+    int jj = 1;
+    while (C2(jj) <= rem) jj++;
+    jj--;
+    rem -= C2(jj);
+    i = (int)rem; j = jj; k = kk; l = ll;
+}
+
+// mc_sparse.cu:477-537 without the dense temporaries: survivors are counted
+// per (l,k) block on the device and the partial Fisher-Yates shuffle runs on
+// a virtual array whose entries are located by rank.
+static int setup_sparse_quartets(pspin_state* s, SampleHost& h, std::vector<QuartetRec>& qs) {
+    const pspin_config& c = h.cfg;
+    const int N = c.N;
+    const double J4 = c.alpha * c.J, J40 = c.alpha0 * c.J0;
+    const int64_t nq = C4(N);
+    SurvivorIndex si;
+    si.N = N;
+    si.fmc = c.fmc_mode;
+    si.gamma = c.gamma;
+    si.w = h.omega.data();
+    if (c.fmc_mode == 0) {
+        si.total = nq;
+    } else {
+        double* d_w = nullptr;
+        unsigned long long* d_cnt = nullptr;
+        TRY(dalloc(&d_w, N));
+        int rc = dalloc(&d_cnt, (size_t)N * N);
+        std::vector<unsigned long long> cnt((size_t)N * N);
+        if (rc == PSPIN_OK) {
+            cudaError_t e = cudaMemcpyAsync(d_w, h.omega.data(), N * sizeof(double), cudaMemcpyHostToDevice, s->st);
+            if (e == cudaSuccess) e = dev_survivor_counts(d_cnt, d_w, N, c.gamma, s->st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(cnt.data(), d_cnt, cnt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+            if (e != cudaSuccess) rc = fail(PSPIN_ERR_CUDA, "survivor count: %s", cudaGetErrorString(e));
+        }
+        cudaFree(d_w);
+        cudaFree(d_cnt);
+        if (rc != PSPIN_OK) return rc;
+        si.pre.push_back(0);
+        for (int l = 3; l < N; l++)
+            for (int k = 2; k < l; k++) {
+                const unsigned long long v = cnt[(size_t)l * N + k];
+                if (!v) continue;
+                si.bl.push_back(l);
+                si.bk.push_back(k);
+                si.pre.push_back(si.pre.back() + (int64_t)v);
+            }
+        si.total = si.pre.back();
+    }
+    h.n_quart_active = si.total;
+    int ns = N;
+    if (si.total < ns) {
+        if (!s->opt.quiet)
+            fprintf(stderr, "WARNING: only %lld non-zero quartets after FMC, requested %d. Using all.\n",
+                    (long long)si.total, ns);
+        ns = (int)si.total;
+    }
+    // partial Fisher-Yates (mc_sparse.cu:340-349) on the virtual survivor array
+    std::unordered_map<int64_t, int64_t> moved;
+    auto get = [&](int64_t i) {
+        auto it = moved.find(i);
+        return it != moved.end() ? it->second : si.at(i);
+    };
+    uint64_t rng = c.seed + 4000;
+    const int64_t count = si.total;
+    for (int i = 0; i < ns && i < (int)count; i++) {
+        const uint64_t r = splitmix64(rng);
+        const int64_t j = i + (int64_t)(r % (uint64_t)(count - i));
+        const int64_t vi = get(i), vj = get(j);
+        moved[i] = vj;
+        moved[j] = vi;
+    }
+    std::vector<int64_t> sel(ns), selq(ns);
+    for (int t = 0; t < ns; t++) {
+        sel[t] = get(t);
+        selq[t] = sel[t] / 3;
+    }
+    // coupling values: the same single cuRAND call as the reference's dense
+    // temporary (mc_sparse.cu:424, disorder.cu:93-106), gathered at the
+    // selected quartets
+    std::vector<double> raw(ns);
+    if (ns > 0) {
+        double* d_nrm = nullptr;
+        int64_t* d_q = nullptr;
+        double* d_out = nullptr;
+        int rc = dalloc(&d_nrm, 2 * (size_t)nq);
+        if (rc != PSPIN_OK)
+            return fail(PSPIN_ERR_ALLOC,
+                        "sparse set-up needs the cuRAND stream of 2*C(N,4) = %lld doubles on the device: %s",
+                        (long long)(2 * nq), g_err.c_str());
+        rc = dalloc(&d_q, ns);
+        if (rc == PSPIN_OK) rc = dalloc(&d_out, ns);
+        if (rc == PSPIN_OK) rc = curand_normals(c.seed + 2000 + 12345, 2 * (size_t)nq, d_nrm, s->st);
+        if (rc == PSPIN_OK) {
+            cudaError_t e = cudaMemcpyAsync(d_q, selq.data(), ns * sizeof(int64_t), cudaMemcpyHostToDevice, s->st);
+            if (e == cudaSuccess) e = dev_gather_real(d_nrm, d_q, ns, d_out, s->st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(raw.data(), d_out, ns * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+            if (e != cudaSuccess) rc = fail(PSPIN_ERR_CUDA, "sparse gather: %s", cudaGetErrorString(e));
+        }
+        cudaFree(d_nrm);
+        cudaFree(d_q);
+        cudaFree(d_out);
+        if (rc != PSPIN_OK) return rc;
+    }
+    const double sigma = J4 * std::sqrt((double)N / (double)(ns > 0 ? ns : 1));
+    const double mean4 = (J40 != 0.0) ? J40 * (double)N / (double)ns : 0.0;
+    h.sq.resize((size_t)ns * 5);
+    h.sqg.resize(ns);
+    qs.clear();
+    for (int t = 0; t < ns; t++) {
+        const int ch = (int)(sel[t] % 3);
+        int i, j, k, l;
+        decode_q(selq[t], i, j, k, l);
+        const double g = raw[t] * sigma + mean4;
+        int32_t* e = &h.sq[(size_t)t * 5];
+        e[0] = i; e[1] = j; e[2] = k; e[3] = l; e[4] = ch;
+        h.sqg[t] = g;
+        qs.push_back(QuartetRec{i, j, k, l, ch, g});
+    }
+    return PSPIN_OK;
+}
+
+// dense g4: generation, FMC mask, popcount, rescale, shift, all on the
+// device (mc.cu:445-446, 480-483, 492, 499-502)
+static int setup_dense_g4(pspin_state* s, SampleHost& h, std::vector<double>& g4re, std::vector<uint8_t>& mask) {
+    const pspin_config& c = h.cfg;
+    const int N = c.N;
+    const int64_t nq = C4(N);
+    const double J4 = c.alpha * c.J, J40 = c.alpha0 * c.J0;
+    double* d_nrm = nullptr;
+    TRY(dalloc(&d_nrm, 2 * (size_t)nq));
+    int rc = curand_normals(c.seed + 2000 + 12345, 2 * (size_t)nq, d_nrm, s->st);
+    double* g4 = s->d_g4re + h.g4_off;
+    uint8_t* m = s->d_mask + h.g4_off;
+    unsigned long long* d_cnt = nullptr;
+    double* d_w = nullptr;
+    if (rc == PSPIN_OK) rc = dalloc(&d_cnt, 1);
+    if (rc == PSPIN_OK && c.fmc_mode > 0) rc = dalloc(&d_w, N);
+    if (rc == PSPIN_OK) {
+        cudaError_t e = cudaSuccess;
+        unsigned long long a = 0;
+        if (c.fmc_mode > 0) {
+            e = cudaMemcpyAsync(d_w, h.omega.data(), N * sizeof(double), cudaMemcpyHostToDevice, s->st);
+            if (e == cudaSuccess) e = dev_fmc_mask(m, d_w, N, c.gamma, s->st);
+            if (e == cudaSuccess) e = dev_popcount(m, nq, d_cnt, s->st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&a, d_cnt, sizeof(a), cudaMemcpyDeviceToHost, s->st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+        } else {
+            e = cudaMemsetAsync(m, 1, (size_t)nq, s->st);
+            a = (unsigned long long)nq;
+        }
+        h.n_quart_active = (int64_t)a;
+        if (e == cudaSuccess) {
+            const double sigma = (a > 0) ? J4 * std::sqrt((double)N / (double)a) : 1.0;
+            const double mean = (J40 != 0.0 && a > 0) ? J40 * (double)N / (double)a : 0.0;
+            e = dev_g4_real(d_nrm, g4, nq, sigma, mean, s->st);
+        }
+        if (e == cudaSuccess) {
+            g4re.resize(nq);
+            mask.resize(nq);
+            e = cudaMemcpyAsync(g4re.data(), g4, nq * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(mask.data(), m, nq, cudaMemcpyDeviceToHost, s->st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+        }
+        if (e != cudaSuccess) rc = fail(PSPIN_ERR_CUDA, "dense g4 set-up: %s", cudaGetErrorString(e));
+    }
+    cudaFree(d_nrm);
+    cudaFree(d_cnt);
+    cudaFree(d_w);
+    return rc;
+}
+
+static int choose_warps(const pspin_state* s) {
+    if (s->opt.warps_per_unit > 0) {
+        int w = s->opt.warps_per_unit;
+        if (w > 8 || (32 % w) != 0) return -1;
+        return w;
+    }
+    double per_site = 0.0;
+    for (const SampleHost& h : s->hs) per_site = std::max(per_site, (double)h.site_entries / h.N);
+    if (per_site > 16000) return 8;
+    if (per_site > 4000) return 4;
+    if (per_site > 1000) return 2;
+    return 1;
+}
+
+static int run_energy(pspin_state* s, double* e2, double* e4, bool overwrite, bool renorm) {
+    EnergyParams p{};
+    p.samples = s->d_samples;
+    p.units = s->d_units;
+    p.spins = s->d_spins;
+    p.quartets = s->d_q64;
+    p.g2 = s->d_g2;
+    p.e2 = e2;
+    p.e4 = e4;
+    p.energy = overwrite ? s->d_E : nullptr;
+    p.drift = overwrite ? s->d_drift : nullptr;
+    p.target = renorm ? s->d_target : nullptr;
+    CK(launch_energy(p, (int)s->units.size(), s->max_N, s->st));
+    s->kernel_launches++;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, const pspin_options* opt,
+                                  pspin_state** out) {
+    if (!cfgs || n <= 0 || !out) return fail(PSPIN_ERR_ARG, "pspin_create_batch: bad arguments");
+    if (variant != PSPIN_DENSE && variant != PSPIN_SPARSE) return fail(PSPIN_ERR_ARG, "unknown variant %d", variant);
+    *out = nullptr;
+    for (int k = 0; k < n; k++) {
+        const pspin_config& c = cfgs[k];
+        if (c.N < 4) return fail(PSPIN_ERR_ARG, "Error: N must be >= 4 for 4-body interactions.");
+        if (c.N > 1000) return fail(PSPIN_ERR_ARG, "N=%d above the engine limit 1000", c.N);
+        if (c.nrep < 1) return fail(PSPIN_ERR_ARG, "nrep must be >= 1");
+        if (c.fmc_mode < 0 || c.fmc_mode > 2) return fail(PSPIN_ERR_ARG, "fmc must be 0, 1 or 2");
+        if (variant == PSPIN_DENSE && C4(c.N) > (int64_t)400000000)
+            return fail(PSPIN_ERR_ARG, "dense variant: C(N,4) too large for N=%d", c.N);
+    }
+    pspin_state* s = new pspin_state();
+    if (opt) s->opt = *opt;
+    else {
+        std::memset(&s->opt, 0, sizeof(s->opt));
+        s->opt.trace_replica = -1;
+    }
+    if (s->opt.resync_every == 0) s->opt.resync_every = 1024;
+    s->variant = variant;
+    s->S = n;
+    s->hs.resize(n);
+    auto bail = [&](int rc) {
+        free_state(s);
+        return rc;
+    };
+    {
+        int dev = cfgs[0].dev;
+        if (dev >= 0) {
+            cudaError_t e = cudaSetDevice(dev);
+            if (e != cudaSuccess) return bail(fail(PSPIN_ERR_CUDA, "cudaSetDevice(%d): %s", dev, cudaGetErrorString(e)));
+        }
+        cudaGetDevice(&s->device);
+        cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return bail(fail(PSPIN_ERR_CUDA, "stream: %s", cudaGetErrorString(e)));
+    }
+
+    // ---- per-sample host descriptors and pools
+    int64_t g4_pool = 0;
+    for (int k = 0; k < n; k++) {
+        SampleHost& h = s->hs[k];
+        h.cfg = cfgs[k];
+        h.N = cfgs[k].N;
+        h.R = cfgs[k].nrep;
+        if (variant == PSPIN_DENSE) {
+            h.g4_off = g4_pool;
+            h.nq_dense = C4(h.N);
+            g4_pool += h.nq_dense;
+        }
+        s->R_tot += h.R;
+        s->max_N = std::max(s->max_N, h.N);
+        s->spin_total += (int64_t)h.N * h.R;
+    }
+    int rc = PSPIN_OK;
+    if (variant == PSPIN_DENSE) {
+        rc = dalloc(&s->d_g4re, (size_t)g4_pool);
+        if (rc == PSPIN_OK) rc = dalloc(&s->d_mask, (size_t)g4_pool);
+        if (rc != PSPIN_OK) return bail(rc);
+    }
+
+    // ---- disorder, spins, layouts
+    std::vector<SiteLists> lists(n);
+    std::vector<std::vector<Q64>> q64(n);
+    std::vector<std::vector<float2>> spins(n);
+    std::vector<std::vector<double>> targets(n);
+    std::vector<std::vector<uint64_t>> keys(n);
+    // phase 1 (device, in sample order): cuRAND streams, FMC masks, survivor
+    // counts, coupling rescale; host copies of what the layout needs
+    std::vector<std::vector<QuartetRec>> qsv(n);
+    std::vector<std::vector<double>> g4h(n), nrmv(n);
+    std::vector<std::vector<uint8_t>> maskh(n);
+    for (int k = 0; k < n; k++) {
+        SampleHost& h = s->hs[k];
+        const int N = h.N, R = h.R;
+        rc = setup_g2(h, s->st);
+        if (rc != PSPIN_OK) return bail(rc);
+        if (variant == PSPIN_DENSE) {
+            rc = setup_dense_g4(s, h, g4h[k], maskh[k]);
+            if (rc != PSPIN_OK) return bail(rc);
+        } else {
+            rc = setup_sparse_quartets(s, h, qsv[k]);
+            if (rc != PSPIN_OK) return bail(rc);
+        }
+        // replica seeds (mc.cu:419-423) double as the Philox move keys (mc.cu:521)
+        keys[k].resize(R);
+        uint64_t master = h.cfg.seed;
+        for (int r = 0; r < R; r++) keys[k][r] = splitmix64(master);
+        // initial amplitudes: cuRAND normals per replica (spins.cu:75-82)
+        std::vector<double>& nrm = nrmv[k];
+        nrm.resize(2 * (size_t)N * R);
+        {
+            double* d = nullptr;
+            rc = dalloc(&d, nrm.size());
+            if (rc != PSPIN_OK) return bail(rc);
+            for (int r = 0; r < R && rc == PSPIN_OK; r++)
+                rc = curand_normals(keys[k][r], 2 * (size_t)N, d + 2 * (size_t)N * r, s->st);
+            if (rc == PSPIN_OK) {
+                cudaError_t e = cudaMemcpyAsync(nrm.data(), d, nrm.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+                if (e != cudaSuccess) rc = fail(PSPIN_ERR_CUDA, "spin init copy: %s", cudaGetErrorString(e));
+            }
+            cudaFree(d);
+            if (rc != PSPIN_OK) return bail(rc);
+        }
+    }
+    // phase 2 (host, samples in parallel): normalisation, quartet lists,
+    // per-site sweep lists, FP64 quartet tables
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < n; k++) {
+        SampleHost& h = s->hs[k];
+        const int N = h.N, R = h.R;
+        if (variant == PSPIN_DENSE) {
+            dense_quartets(N, g4h[k].data(), maskh[k].data(), qsv[k]);
+            std::vector<double>().swap(g4h[k]);
+            std::vector<uint8_t>().swap(maskh[k]);
+        }
+        targets[k].resize(R);
+        spins[k].resize((size_t)N * R);
+        for (int r = 0; r < R; r++) {
+            double* sp = nrmv[k].data() + 2 * (size_t)N * r;
+            targets[k][r] = normalize_host(sp, N, variant == PSPIN_SPARSE, s->opt.init_exact);
+            for (int i = 0; i < N; i++)
+                spins[k][(size_t)i * R + r] = make_float2((float)sp[2 * i], (float)sp[2 * i + 1]);
+        }
+        std::vector<double>().swap(nrmv[k]);
+        build_site_lists(N, h.g2re.data(), h.h2_active, qsv[k], lists[k]);
+        build_q64(qsv[k], q64[k]);
+        std::vector<QuartetRec>().swap(qsv[k]);
+        h.site_entries = (int64_t)lists[k].entries.size();
+    }
+
+    // ---- concatenate and upload
+    int64_t ent_total = 0, split_total = 0, q_total = 0, g2_total = 0, spin_off = 0, rep_off = 0, chunk_total = 0;
+    s->sd.resize(n);
+    for (int k = 0; k < n; k++) {
+        SampleHost& h = s->hs[k];
+        SampleDev& d = s->sd[k];
+        d.N = h.N;
+        d.R = h.R;
+        d.h2_active = h.h2_active;
+        d.variant = variant;
+        d.spin_off = spin_off;
+        d.rep_off = rep_off;
+        d.split_off = split_total;
+        d.q_off = q_total;
+        d.nq = (int64_t)q64[k].size();
+        d.g2_off = g2_total;
+        uint64_t pk = h.cfg.seed + 7000;
+        const uint64_t key = splitmix64(pk);
+        d.pair_key0 = (uint32_t)key;
+        d.pair_key1 = (uint32_t)(key >> 32);
+        spin_off += (int64_t)h.N * h.R;
+        rep_off += h.R;
+        split_total += (int64_t)h.N * (kSplit + 1);
+        q_total += d.nq;
+        g2_total += (int64_t)h.N * h.N;
+        ent_total += h.site_entries;
+        chunk_total += (int64_t)lists[k].chunk_start.size();
+    }
+    if (chunk_total >= (1ll << 31)) return bail(fail(PSPIN_ERR_ARG, "too many list chunks"));
+    std::vector<int2> ent(ent_total);
+    std::vector<int> site_chunks(split_total);
+    std::vector<int64_t> chunk_start(chunk_total + 1);
+    std::vector<Q64> qall(q_total);
+    std::vector<double> g2all(g2_total);
+    std::vector<float2> spall(s->spin_total);
+    std::vector<double> tall(s->R_tot), Eall(s->R_tot, 0.0);
+    std::vector<uint64_t> kall(s->R_tot);
+    {
+        int64_t eoff = 0, coff = 0;
+        for (int k = 0; k < n; k++) {
+            const SampleDev& d = s->sd[k];
+            std::copy(lists[k].entries.begin(), lists[k].entries.end(), ent.begin() + eoff);
+            for (size_t t = 0; t < lists[k].chunk_start.size(); t++) chunk_start[coff + t] = lists[k].chunk_start[t] + eoff;
+            for (size_t t = 0; t < lists[k].site_chunks.size(); t++)
+                site_chunks[d.split_off + t] = (int)(lists[k].site_chunks[t] + coff);
+            eoff += (int64_t)lists[k].entries.size();
+            coff += (int64_t)lists[k].chunk_start.size();
+            std::copy(q64[k].begin(), q64[k].end(), qall.begin() + d.q_off);
+            std::copy(s->hs[k].g2re.begin(), s->hs[k].g2re.end(), g2all.begin() + d.g2_off);
+            std::copy(spins[k].begin(), spins[k].end(), spall.begin() + d.spin_off);
+            std::copy(targets[k].begin(), targets[k].end(), tall.begin() + d.rep_off);
+            std::copy(keys[k].begin(), keys[k].end(), kall.begin() + d.rep_off);
+            lists[k] = SiteLists();
+            q64[k].clear();
+        }
+        chunk_start[chunk_total] = eoff;
+    }
+    // units: replica blocks of 32, heaviest samples first
+    for (int k = 0; k < n; k++)
+        for (int rb = 0; rb < s->hs[k].R; rb += kRepBlock)
+            s->units.push_back(Unit{k, rb, std::min(kRepBlock, s->hs[k].R - rb), 0});
+    std::stable_sort(s->units.begin(), s->units.end(), [&](const Unit& a, const Unit& b) {
+        return s->hs[a.sample].site_entries > s->hs[b.sample].site_entries;
+    });
+    s->warps = choose_warps(s);
+    if (s->warps < 0) return bail(fail(PSPIN_ERR_ARG, "warps_per_unit must be 1, 2, 4 or 8"));
+    if (sweep_smem_bytes(s->max_N, s->warps) > 227 * 1024)
+        return bail(fail(PSPIN_ERR_ARG, "N=%d needs more shared memory than a CTA has", s->max_N));
+
+    if ((rc = dalloc(&s->d_samples, n)) || (rc = dalloc(&s->d_units, s->units.size())) ||
+        (rc = dalloc(&s->d_spins, (size_t)s->spin_total)) || (rc = dalloc(&s->d_E, s->R_tot)) ||
+        (rc = dalloc(&s->d_beta, s->R_tot)) || (rc = dalloc(&s->d_target, s->R_tot)) ||
+        (rc = dalloc(&s->d_drift, s->R_tot)) || (rc = dalloc(&s->d_e2, s->R_tot)) ||
+        (rc = dalloc(&s->d_e4, s->R_tot)) || (rc = dalloc(&s->d_acc, s->R_tot)) ||
+        (rc = dalloc(&s->d_prop, s->R_tot)) || (rc = dalloc(&s->d_key, s->R_tot)) ||
+        (rc = dalloc(&s->d_entries, (size_t)ent_total)) || (rc = dalloc(&s->d_site_chunks, (size_t)split_total)) ||
+        (rc = dalloc(&s->d_chunk_start, (size_t)chunk_total + 1)) ||
+        (rc = dalloc(&s->d_q64, (size_t)std::max<int64_t>(q_total, 1))) ||
+        (rc = dalloc(&s->d_g2, (size_t)g2_total)) || (rc = dalloc(&s->d_sweep_counter, 1)) ||
+        (rc = dalloc(&s->d_status, 1)))
+        return bail(rc);
+    auto up = [&](void* dst, const void* src, size_t bytes) -> int {
+        if (!bytes) return PSPIN_OK;
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->st);
+        if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+        return PSPIN_OK;
+    };
+    std::vector<double> ones(s->R_tot);
+    for (int k = 0; k < n; k++)
+        for (int r = 0; r < s->hs[k].R; r++) ones[s->sd[k].rep_off + r] = 1.0 / s->hs[k].cfg.T;
+    if ((rc = up(s->d_samples, s->sd.data(), n * sizeof(SampleDev))) ||
+        (rc = up(s->d_units, s->units.data(), s->units.size() * sizeof(Unit))) ||
+        (rc = up(s->d_spins, spall.data(), spall.size() * sizeof(float2))) ||
+        (rc = up(s->d_target, tall.data(), tall.size() * sizeof(double))) ||
+        (rc = up(s->d_key, kall.data(), kall.size() * sizeof(uint64_t))) ||
+        (rc = up(s->d_entries, ent.data(), ent.size() * sizeof(int2))) ||
+        (rc = up(s->d_site_chunks, site_chunks.data(), site_chunks.size() * sizeof(int))) ||
+        (rc = up(s->d_chunk_start, chunk_start.data(), chunk_start.size() * sizeof(int64_t))) ||
+        (rc = up(s->d_q64, qall.data(), qall.size() * sizeof(Q64))) ||
+        (rc = up(s->d_g2, g2all.data(), g2all.size() * sizeof(double))) ||
+        (rc = up(s->d_beta, ones.data(), ones.size() * sizeof(double))))
+        return bail(rc);
+    {
+        cudaError_t e = cudaMemsetAsync(s->d_acc, 0, s->R_tot * sizeof(long long), s->st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->d_prop, 0, s->R_tot * sizeof(long long), s->st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->d_E, 0, s->R_tot * sizeof(double), s->st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->d_sweep_counter, 0, sizeof(long long), s->st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->d_status, 0, sizeof(int), s->st);
+        if (e != cudaSuccess) return bail(fail(PSPIN_ERR_CUDA, "memset: %s", cudaGetErrorString(e)));
+    }
+    if (s->opt.trace_replica >= 0 && s->opt.trace_capacity > 0) {
+        if ((rc = dalloc(&s->d_trace, (size_t)s->opt.trace_capacity))) return bail(rc);
+        cudaMemsetAsync(s->d_trace, 0, sizeof(pspin_move_record) * (size_t)s->opt.trace_capacity, s->st);
+    }
+    // initial energies (the chain's form, FP64, from the FP32 amplitudes)
+    if ((rc = run_energy(s, nullptr, nullptr, true, false))) return bail(rc);
+    {
+        cudaError_t e = cudaStreamSynchronize(s->st);
+        if (e != cudaSuccess) return bail(fail(PSPIN_ERR_CUDA, "init: %s", cudaGetErrorString(e)));
+    }
+    *out = s;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_create(const pspin_config* cfg, int variant, const pspin_options* opt, pspin_state** out) {
+    return pspin_create_batch(cfg, 1, variant, opt, out);
+}
+
+extern "C" int pspin_destroy(pspin_state* s) {
+    if (!s) return PSPIN_OK;
+    cudaStreamSynchronize(s->st);
+    free_state(s);
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_total_replicas(const pspin_state* s) { return s ? s->R_tot : 0; }
+extern "C" int pspin_num_samples(const pspin_state* s) { return s ? s->S : 0; }
+
+// ------------------------------------------------------------------ sweeps
+static int launch_chunk(pspin_state* s, int nsweeps, bool exchange) {
+    SweepParams p{};
+    p.samples = s->d_samples;
+    p.units = s->d_units;
+    p.spins = s->d_spins;
+    p.energy = s->d_E;
+    p.accepted = s->d_acc;
+    p.proposed = s->d_prop;
+    p.beta = s->d_beta;
+    p.key = s->d_key;
+    p.entries = s->d_entries;
+    p.chunk_start = s->d_chunk_start;
+    p.site_chunks = s->d_site_chunks;
+    p.sweep_counter = s->d_sweep_counter;
+    p.nsweeps = nsweeps;
+    p.warps = s->warps;
+    p.trace_sample = s->opt.trace_sample;
+    p.trace_rep = s->opt.trace_replica;
+    p.trace_cap = s->opt.trace_capacity;
+    p.trace_sweep0 = s->trace_sweep0;
+    p.trace = s->d_trace;
+    p.status = s->d_status;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (s->profiling) {
+        if (s->ev_used == s->ev_pool.size()) {
+            std::pair<cudaEvent_t, cudaEvent_t> pr;
+            CK(cudaEventCreate(&pr.first));
+            CK(cudaEventCreate(&pr.second));
+            s->ev_pool.push_back(pr);
+        }
+        e0 = s->ev_pool[s->ev_used].first;
+        e1 = s->ev_pool[s->ev_used].second;
+        s->ev_used++;
+        CK(cudaEventRecord(e0, s->st));
+    }
+    CK(launch_sweep(p, (int)s->units.size(), s->variant, s->max_N, s->st));
+    if (s->profiling) CK(cudaEventRecord(e1, s->st));
+    s->sweep_launches++;
+    s->kernel_launches++;
+    ExchangeParams x{};
+    x.n_samples = s->S;
+    x.NT = s->pt_NT;
+    x.nrep = s->pt_nrep;
+    x.samples = s->d_samples;
+    x.beta_sched = s->d_beta_sched;
+    x.energy = s->d_E;
+    x.beta = s->d_beta;
+    x.perm = s->d_perm;
+    x.drand_state = s->d_drand;
+    x.ex_acc = s->d_ex_acc;
+    x.ex_prop = s->d_ex_prop;
+    x.sweep_counter = s->d_sweep_counter;
+    x.nsweeps_done = nsweeps;
+    x.do_exchange = exchange ? 1 : 0;
+    CK(launch_exchange(x, s->st));
+    s->kernel_launches++;
+    s->sweeps_done += nsweeps;
+    s->since_resync += nsweeps;
+    if (s->opt.resync_every > 0 && s->since_resync >= s->opt.resync_every) {
+        TRY(run_energy(s, nullptr, nullptr, true, true));
+        s->since_resync = 0;
+    }
+    return PSPIN_OK;
+}
+
+static int run_sweeps(pspin_state* s, int nsweeps, bool pt) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (nsweeps < 0) return fail(PSPIN_ERR_ARG, "nsweeps < 0");
+    int left = nsweeps;
+    while (left > 0) {
+        int chunk = left;
+        if (s->opt.resync_every > 0) chunk = std::min<long long>(chunk, s->opt.resync_every - s->since_resync);
+        bool ex = false;
+        if (pt) {
+            const int to_ex = s->pt_freq - (int)(s->sweeps_done % s->pt_freq);
+            if (to_ex <= chunk) {
+                chunk = to_ex;
+                ex = true;
+            }
+        }
+        if (chunk <= 0) chunk = 1;
+        TRY(launch_chunk(s, chunk, ex));
+        left -= chunk;
+    }
+    CK(cudaStreamSynchronize(s->st));
+    int status = 0;
+    CK(cudaMemcpy(&status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) return fail(PSPIN_ERR_TIMEOUT, "a bounded wait in the sweep kernel expired (status %d)", status);
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_sweep(pspin_state* s, int nsweeps) { return run_sweeps(s, nsweeps, false); }
+
+extern "C" int pspin_set_betas(pspin_state* s, const double* betas) {
+    if (!s || !betas) return fail(PSPIN_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(s->d_beta, betas, s->R_tot * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_fill_betas(pspin_state* s, double beta) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    std::vector<double> b(s->R_tot, beta);
+    return pspin_set_betas(s, b.data());
+}
+
+extern "C" int pspin_get_results(pspin_state* s, double* E, int64_t* acc, int64_t* prop) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (E) CK(cudaMemcpyAsync(E, s->d_E, s->R_tot * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    if (acc) CK(cudaMemcpyAsync(acc, s->d_acc, s->R_tot * sizeof(long long), cudaMemcpyDeviceToHost, s->st));
+    if (prop) CK(cudaMemcpyAsync(prop, s->d_prop, s->R_tot * sizeof(long long), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_reset_counters(pspin_state* s) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    CK(cudaMemsetAsync(s->d_acc, 0, s->R_tot * sizeof(long long), s->st));
+    CK(cudaMemsetAsync(s->d_prop, 0, s->R_tot * sizeof(long long), s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_get_spins(pspin_state* s, double* out) {
+    if (!s || !out) return fail(PSPIN_ERR_ARG, "null argument");
+    std::vector<float2> h(s->spin_total);
+    CK(cudaMemcpyAsync(h.data(), s->d_spins, h.size() * sizeof(float2), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (int k = 0; k < s->S; k++) {
+        const SampleDev& d = s->sd[k];
+        for (int r = 0; r < d.R; r++)
+            for (int i = 0; i < d.N; i++) {
+                const float2 v = h[d.spin_off + (int64_t)i * d.R + r];
+                double* o = out + 2 * ((int64_t)d.N * (d.rep_off + r) - (int64_t)d.N * d.rep_off + d.spin_off) + 2 * i;
+                o[0] = v.x;
+                o[1] = v.y;
+            }
+    }
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_set_spins(pspin_state* s, const double* in) {
+    if (!s || !in) return fail(PSPIN_ERR_ARG, "null argument");
+    std::vector<float2> h(s->spin_total);
+    for (int k = 0; k < s->S; k++) {
+        const SampleDev& d = s->sd[k];
+        for (int r = 0; r < d.R; r++)
+            for (int i = 0; i < d.N; i++) {
+                const double* o = in + 2 * (d.spin_off + (int64_t)d.N * r) + 2 * i;
+                h[d.spin_off + (int64_t)i * d.R + r] = make_float2((float)o[0], (float)o[1]);
+            }
+    }
+    CK(cudaMemcpyAsync(s->d_spins, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice, s->st));
+    TRY(run_energy(s, nullptr, nullptr, true, false));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_split_energies(pspin_state* s, double* e2, double* e4) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    TRY(run_energy(s, s->d_e2, s->d_e4, false, false));
+    if (e2) CK(cudaMemcpyAsync(e2, s->d_e2, s->R_tot * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    if (e4) CK(cudaMemcpyAsync(e4, s->d_e4, s->R_tot * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_resync(pspin_state* s) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    TRY(run_energy(s, nullptr, nullptr, true, true));
+    s->since_resync = 0;
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+// ------------------------------------------------------------------ introspection
+extern "C" int pspin_get_info(pspin_state* s, int sample, pspin_info* info) {
+    if (!s || !info || sample < 0 || sample >= s->S) return fail(PSPIN_ERR_ARG, "bad arguments");
+    const SampleHost& h = s->hs[sample];
+    info->N = h.N;
+    info->nrep = h.R;
+    info->h2_active = h.h2_active;
+    info->n_quartets = (int)(h.sqg.size());
+    info->n_pairs_active = h.n_pairs_active;
+    info->n_quart_active = h.n_quart_active;
+    info->site_entries = h.site_entries;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_get_omega(pspin_state* s, int sample, double* omega) {
+    if (!s || !omega || sample < 0 || sample >= s->S) return fail(PSPIN_ERR_ARG, "bad arguments");
+    const SampleHost& h = s->hs[sample];
+    if (h.omega.empty()) return fail(PSPIN_ERR_STATE, "fully connected sample has no frequencies");
+    std::copy(h.omega.begin(), h.omega.end(), omega);
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_get_couplings(pspin_state* s, int sample, double* g2, double* g4, uint8_t* mask) {
+    if (!s || sample < 0 || sample >= s->S) return fail(PSPIN_ERR_ARG, "bad arguments");
+    const SampleHost& h = s->hs[sample];
+    if (g2)
+        for (size_t t = 0; t < h.g2re.size(); t++) { g2[2 * t] = h.g2re[t]; g2[2 * t + 1] = 0.0; }
+    if (g4 || mask) {
+        if (s->variant != PSPIN_DENSE) return fail(PSPIN_ERR_STATE, "sparse variant keeps no dense g4");
+        if (g4) {
+            std::vector<double> t(h.nq_dense);
+            CK(cudaMemcpyAsync(t.data(), s->d_g4re + h.g4_off, h.nq_dense * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+            for (int64_t q = 0; q < h.nq_dense; q++) { g4[2 * q] = t[q]; g4[2 * q + 1] = 0.0; }
+        }
+        if (mask) {
+            CK(cudaMemcpyAsync(mask, s->d_mask + h.g4_off, h.nq_dense, cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+        }
+    }
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_get_sparse_quartets(pspin_state* s, int sample, int32_t* ijklch, double* g) {
+    if (!s || sample < 0 || sample >= s->S) return fail(PSPIN_ERR_ARG, "bad arguments");
+    const SampleHost& h = s->hs[sample];
+    if (s->variant != PSPIN_SPARSE) return fail(PSPIN_ERR_STATE, "dense variant has no sparse quartet list");
+    if (ijklch) std::copy(h.sq.begin(), h.sq.end(), ijklch);
+    if (g) std::copy(h.sqg.begin(), h.sqg.end(), g);
+    return PSPIN_OK;
+}
+
+// ------------------------------------------------------------------ parallel tempering
+extern "C" int pspin_pt_init(pspin_state* s, int NT, int nrep, const double* beta_sched, int pt_freq) {
+    if (!s || !beta_sched) return fail(PSPIN_ERR_ARG, "null argument");
+    if (NT < 2 || nrep < 1 || pt_freq < 1) return fail(PSPIN_ERR_ARG, "need NT >= 2, nrep >= 1, pt_freq >= 1");
+    for (const SampleHost& h : s->hs)
+        if (h.R != NT * nrep) return fail(PSPIN_ERR_ARG, "sample nrep %d != NT*nrep_per_temp %d", h.R, NT * nrep);
+    cudaFree(s->d_beta_sched);
+    cudaFree(s->d_perm);
+    cudaFree(s->d_drand);
+    cudaFree(s->d_ex_acc);
+    cudaFree(s->d_ex_prop);
+    s->d_beta_sched = nullptr; s->d_perm = nullptr; s->d_drand = nullptr; s->d_ex_acc = nullptr; s->d_ex_prop = nullptr;
+    s->pt_NT = NT;
+    s->pt_nrep = nrep;
+    s->pt_freq = pt_freq;
+    int rc;
+    if ((rc = dalloc(&s->d_beta_sched, NT)) || (rc = dalloc(&s->d_perm, (size_t)s->S * NT * nrep)) ||
+        (rc = dalloc(&s->d_drand, s->S)) || (rc = dalloc(&s->d_ex_acc, (size_t)s->S * (NT - 1))) ||
+        (rc = dalloc(&s->d_ex_prop, (size_t)s->S * (NT - 1))))
+        return rc;
+    std::vector<int> perm((size_t)s->S * NT * nrep);
+    std::vector<unsigned long long> dr(s->S);
+    std::vector<double> betas(s->R_tot);
+    for (int k = 0; k < s->S; k++) {
+        for (int i = 0; i < NT * nrep; i++) perm[(size_t)k * NT * nrep + i] = i;   // :283-284
+        dr[k] = srand48_state((long)s->hs[k].cfg.seed + 5000);                        // :304
+        for (int t = 0; t < NT; t++)
+            for (int r = 0; r < nrep; r++) betas[s->sd[k].rep_off + t * nrep + r] = beta_sched[t];  // :274-278
+    }
+    CK(cudaMemcpyAsync(s->d_beta_sched, beta_sched, NT * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->d_perm, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->d_drand, dr.data(), dr.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemsetAsync(s->d_ex_acc, 0, (size_t)s->S * (NT - 1) * sizeof(long long), s->st));
+    CK(cudaMemsetAsync(s->d_ex_prop, 0, (size_t)s->S * (NT - 1) * sizeof(long long), s->st));
+    CK(cudaMemcpyAsync(s->d_beta, betas.data(), betas.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_pt_run(pspin_state* s, int nsweeps) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (s->pt_NT < 2) return fail(PSPIN_ERR_STATE, "pspin_pt_init has not been called");
+    return run_sweeps(s, nsweeps, true);
+}
+
+extern "C" int pspin_pt_get(pspin_state* s, int sample, int32_t* perm, int64_t* ex_acc, int64_t* ex_prop) {
+    if (!s || sample < 0 || sample >= s->S) return fail(PSPIN_ERR_ARG, "bad arguments");
+    if (s->pt_NT < 2) return fail(PSPIN_ERR_STATE, "pspin_pt_init has not been called");
+    const int NT = s->pt_NT, nr = s->pt_nrep;
+    if (perm) CK(cudaMemcpyAsync(perm, s->d_perm + (size_t)sample * NT * nr, NT * nr * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    if (ex_acc) CK(cudaMemcpyAsync(ex_acc, s->d_ex_acc + (size_t)sample * (NT - 1), (NT - 1) * sizeof(long long), cudaMemcpyDeviceToHost, s->st));
+    if (ex_prop) CK(cudaMemcpyAsync(ex_prop, s->d_ex_prop + (size_t)sample * (NT - 1), (NT - 1) * sizeof(long long), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_pt_sweeps_done(pspin_state* s, int64_t* sweeps) {
+    if (!s || !sweeps) return fail(PSPIN_ERR_ARG, "null argument");
+    *sweeps = s->sweeps_done;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_trace_get(pspin_state* s, pspin_move_record* out, int max_records, int* n_records) {
+    if (!s || !out || !n_records) return fail(PSPIN_ERR_ARG, "null argument");
+    if (!s->d_trace) return fail(PSPIN_ERR_STATE, "tracing was not enabled at creation");
+    const int sample = s->opt.trace_sample;
+    const int steps = s->hs[sample].N / 2;
+    long long n = (s->sweeps_done - s->trace_sweep0) * steps;
+    if (n > s->opt.trace_capacity) n = s->opt.trace_capacity;
+    if (n > max_records) n = max_records;
+    CK(cudaMemcpyAsync(out, s->d_trace, (size_t)n * sizeof(pspin_move_record), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    *n_records = (int)n;
+    return PSPIN_OK;
+}
+
+// ------------------------------------------------------------------ stand-alone kernels
+extern "C" int pspin_fmc_mask(int N, const double* omega, double gamma, uint8_t* mask_out, int64_t* n_active) {
+    if (N < 4 || !omega) return fail(PSPIN_ERR_ARG, "bad arguments");
+    const int64_t nq = C4(N);
+    double* d_w = nullptr;
+    uint8_t* d_m = nullptr;
+    unsigned long long* d_c = nullptr;
+    int rc;
+    if ((rc = dalloc(&d_w, N)) || (rc = dalloc(&d_m, (size_t)nq)) || (rc = dalloc(&d_c, 1))) {
+        cudaFree(d_w); cudaFree(d_m); cudaFree(d_c);
+        return rc;
+    }
+    unsigned long long cnt = 0;
+    cudaError_t e = cudaMemcpy(d_w, omega, N * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = dev_fmc_mask(d_m, d_w, N, gamma, 0);
+    if (e == cudaSuccess) e = dev_popcount(d_m, nq, d_c, 0);
+    if (e == cudaSuccess && mask_out) e = cudaMemcpy(mask_out, d_m, (size_t)nq, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&cnt, d_c, sizeof(cnt), cudaMemcpyDeviceToHost);
+    cudaFree(d_w); cudaFree(d_m); cudaFree(d_c);
+    if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "fmc mask: %s", cudaGetErrorString(e));
+    if (n_active) *n_active = (int64_t)cnt;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_quartet_roundtrip(int N, int64_t* n_fail) {
+    if (N < 4 || !n_fail) return fail(PSPIN_ERR_ARG, "bad arguments");
+    unsigned long long* d = nullptr;
+    TRY(dalloc(&d, 1));
+    unsigned long long h = 0;
+    cudaError_t e = dev_roundtrip(N, C4(N), d, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "roundtrip: %s", cudaGetErrorString(e));
+    *n_fail = (int64_t)h;
+    return PSPIN_OK;
+}
+
+// ------------------------------------------------------------------ measurement
+extern "C" void* pspin_stream(pspin_state* s) { return s ? (void*)s->st : nullptr; }
+
+extern "C" int pspin_set_profiling(pspin_state* s, int on) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    s->profiling = on != 0;
+    s->ev_used = 0;
+    s->sweep_launches = 0;
+    s->kernel_launches = 0;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_get_profile(pspin_state* s, double* ms, int64_t* sweep_launches, int64_t* kernel_launches) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    CK(cudaStreamSynchronize(s->st));
+    double tot = 0.0;
+    for (size_t i = 0; i < s->ev_used; i++) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, s->ev_pool[i].first, s->ev_pool[i].second));
+        tot += t;
+    }
+    if (ms) *ms = tot;
+    if (sweep_launches) *sweep_launches = s->sweep_launches;
+    if (kernel_launches) *kernel_launches = s->kernel_launches;
+    s->ev_used = 0;
+    s->sweep_launches = 0;
+    s->kernel_launches = 0;
+    return PSPIN_OK;
+}
+
+namespace pspin {
+cudaError_t launch_fma_probe(float* out, int blocks, int iters, cudaStream_t st);
+}
+
+extern "C" int pspin_fp32_peak(double* tflops) {
+    if (!tflops) return fail(PSPIN_ERR_ARG, "null argument");
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    float* d = nullptr;
+    TRY(dalloc(&d, (size_t)sms * 8 * 1024));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int iters = 1 << 14;
+    const int blocks = sms * 8;
+    cudaError_t e = launch_fma_probe(d, blocks, iters, 0);   // warm-up
+    float best = 1e30f;
+    for (int rep = 0; rep < 5 && e == cudaSuccess; rep++) {
+        cudaEventRecord(a, 0);
+        e = launch_fma_probe(d, blocks, iters, 0);
+        cudaEventRecord(b, 0);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        if (t > 0.f && t < best) best = t;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "fma probe: %s", cudaGetErrorString(e));
+    // 256 threads x 8 independent chains x 2 flop per FMA x iters
+    const double flops = (double)blocks * 256 * 8 * 2.0 * iters;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return PSPIN_OK;
+}
+
+extern "C" const char* pspin_last_error(void) { return g_err.c_str(); }
+extern "C" const char* pspin_version(void) { return "pspin-b200 0.1 (sm_100a)"; }

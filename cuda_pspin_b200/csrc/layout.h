@@ -1,0 +1,27 @@
+// layout.h -- host builders for the sweep's site lists and the FP64 quartet table.
+#pragma once
+#include <vector>
+#include <cstdint>
+#include "internal.h"
+
+namespace pspin {
+
+struct QuartetRec {
+    int i, j, k, l;   // sorted
+    int ch;           // 0, 1, 2
+    double g;         // rescaled coupling (real)
+};
+
+struct SiteLists {
+    std::vector<int2> entries;         // sample-relative
+    std::vector<int64_t> chunk_start;  // sample-relative entry offset of each chunk (no sentinel)
+    std::vector<int> site_chunks;      // N*(kSplit+1) sample-relative chunk indices
+};
+
+void build_site_lists(int N, const double* g2re, int h2_active, const std::vector<QuartetRec>& qs,
+                      SiteLists& out);
+void build_q64(const std::vector<QuartetRec>& qs, std::vector<Q64>& out);
+// every active (q, ch) of a dense mask in q order
+void dense_quartets(int N, const double* g4re, const uint8_t* mask, std::vector<QuartetRec>& out);
+
+}  // namespace pspin

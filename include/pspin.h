@@ -1,0 +1,187 @@
+/*
+ * pspin.h -- C ABI of the B200 engine for the complex 2+4 p-spin glass.
+ *
+ * One opaque handle (pspin_state) owns a batch of disorder samples, each
+ * with its own N, seed and replicas, resident on one GPU.  A batch of one
+ * sample is the reference's MCState / MCStateSparse.  Every entry point
+ * returns PSPIN_OK or an error code; pspin_last_error() gives the message.
+ * Nothing here calls exit().  Calls on one handle must come from one host
+ * thread at a time.  Every call is synchronous with respect to the host
+ * unless stated otherwise.
+ *
+ * Reference interface replaced (giacomotrinca/cuda_pspin), C++ linkage
+ * there, extern "C" here:
+ *   config.h:9-46, config.cu:6-70   SimConfig, default_config, parse_args
+ *   mc.h:33-56                      mc_init, mc_free, mc_sweep, mc_sweep_pt,
+ *                                   mc_set_betas, mc_get_results, mc_get_spins,
+ *                                   mc_compute_split_energies
+ *   mc_sparse.h:42-61               the mc_sparse_* twins
+ *   parallel_tempering.cu:316-352   host replica exchange (here on the device)
+ *   disorder.h:48-69, disorder.cu   FMC filters and survivor counting
+ */
+#ifndef PSPIN_H
+#define PSPIN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------- */
+enum {
+    PSPIN_OK = 0,
+    PSPIN_ERR_ARG = 1,       /* invalid argument (bad N, null pointer, ...)  */
+    PSPIN_ERR_CUDA = 2,      /* a CUDA runtime call failed                   */
+    PSPIN_ERR_CURAND = 3,    /* a cuRAND call failed                         */
+    PSPIN_ERR_ALLOC = 4,     /* device or host allocation failed             */
+    PSPIN_ERR_STATE = 5,     /* call not valid in the handle's current state */
+    PSPIN_ERR_NUMERIC = 6,   /* running energy left the FP64 resync tolerance */
+    PSPIN_ERR_UNSUPPORTED = 7,
+    PSPIN_ERR_TIMEOUT = 8    /* a bounded device wait expired; results invalid */
+};
+
+enum { PSPIN_DENSE = 0,      /* spherical constraint, dense 3-channel H4 (mc.cu)   */
+       PSPIN_SPARSE = 1 };   /* smoothed-cube constraint, N sampled quartets (mc_sparse.cu) */
+
+/* Same field order, types and meaning as the reference's SimConfig
+ * (config.h:9-25), so a SimConfig can be passed by address. */
+typedef struct pspin_config {
+    int save_freq;
+    int verbose;
+    int N;
+    int nrep;            /* replicas in this sample (NT*nrep for PT) */
+    double T;
+    double J;
+    double J0;
+    double alpha;
+    double alpha0;
+    int mc_iterations;
+    uint64_t seed;
+    int label;
+    int dev;
+    int fmc_mode;        /* 0 fully connected, 1 comb, 2 uniform */
+    double gamma;
+} pspin_config;
+
+/* Engine options with no reference counterpart.  Zero-initialised means
+ * the defaults (reference-compatible init, resync every 1024 sweeps). */
+typedef struct pspin_options {
+    int init_exact;      /* 1: full-sum spin normalisation; 0 (default): the
+                            reference's shared-memory tree (spins.cu:27-69),
+                            which drops terms for N not a power of two */
+    int resync_every;    /* FP64 energy resync + renormalisation period in
+                            sweeps (0 -> 1024, <0 -> never) */
+    int warps_per_unit;  /* warps sharing one replica block's move; 0 -> auto */
+    int trace_sample;    /* record every move of one replica (tests): sample */
+    int trace_replica;   /*   ... physical replica; <0 disables tracing */
+    int trace_capacity;  /*   ... number of move records kept */
+    int quiet;           /* suppress the reference's stdout lines */
+    int reserved[7];
+} pspin_options;
+
+typedef struct pspin_info {
+    int N;
+    int nrep;
+    int h2_active;
+    int n_quartets;          /* sparse: selected quartets (= N unless fewer survive) */
+    int64_t n_pairs_active;  /* g2 non-zeros over i<=j (mc.cu:469-477) */
+    int64_t n_quart_active;  /* dense: popcount of the FMC mask; sparse: survivors */
+    int64_t site_entries;    /* entries in the per-site sweep lists */
+} pspin_info;
+
+/* One recorded move of the traced replica (for per-move dE checks). */
+typedef struct pspin_move_record {
+    int32_t i0, j0;          /* pair, i0 < j0 */
+    float ai_old[2], aj_old[2];
+    float ai_new[2], aj_new[2];
+    float dE;                /* FP32 dE the kernel accepted or rejected on */
+    int32_t accepted;
+} pspin_move_record;
+
+typedef struct pspin_state pspin_state;
+
+/* ---- configuration (config.h:28-46, config.cu:6-70) --------------- */
+void pspin_default_config(pspin_config* cfg);
+/* Parses the reference flags into *cfg.  Returns PSPIN_ERR_ARG (and an
+ * error message with the usage line) where the reference calls exit(1). */
+int  pspin_parse_args(int argc, char** argv, pspin_config* cfg);
+
+/* ---- lifetime (mc_init / mc_sparse_init / mc_free) ------------------- */
+int  pspin_create(const pspin_config* cfg, int variant, const pspin_options* opt,
+                  pspin_state** out);
+/* A batch of independent disorder samples in one handle (each cfg its own
+ * N, seed, nrep, FMC).  Sample k's replicas follow sample k-1's in every
+ * per-replica array. */
+int  pspin_create_batch(const pspin_config* cfgs, int n_samples, int variant,
+                        const pspin_options* opt, pspin_state** out);
+int  pspin_destroy(pspin_state* s);
+
+/* ---- sweep interface (mc_sweep_pt, mc_set_betas, ...) -------------- */
+int  pspin_set_betas(pspin_state* s, const double* betas);      /* [total replicas] */
+int  pspin_fill_betas(pspin_state* s, double beta);             /* mc_sweep's 1/T fill */
+int  pspin_sweep(pspin_state* s, int nsweeps);                  /* nsweeps x mc_sweep_pt */
+int  pspin_get_results(pspin_state* s, double* energies, int64_t* accepted, int64_t* proposed);
+int  pspin_reset_counters(pspin_state* s);
+int  pspin_get_spins(pspin_state* s, double* spins);             /* [rep][N][re,im] FP64 */
+int  pspin_set_spins(pspin_state* s, const double* spins);       /* recomputes energies */
+int  pspin_split_energies(pspin_state* s, double* e2, double* e4); /* FP64 from the spins */
+int  pspin_resync(pspin_state* s);   /* FP64 energy recompute + constraint renormalisation */
+int  pspin_total_replicas(const pspin_state* s);
+int  pspin_num_samples(const pspin_state* s);
+
+/* ---- disorder introspection (MCState fields read by the drivers) ---- */
+int  pspin_get_info(pspin_state* s, int sample, pspin_info* info);
+int  pspin_get_omega(pspin_state* s, int sample, double* omega); /* [N]; ERR_STATE if FC */
+int  pspin_get_couplings(pspin_state* s, int sample, double* g2 /*[N*N*2]*/,
+                         double* g4 /*[C(N,4)*2] or NULL*/, uint8_t* mask /*[C(N,4)] or NULL*/);
+int  pspin_get_sparse_quartets(pspin_state* s, int sample, int32_t* ijklch /*[n][5]*/, double* g);
+
+/* ---- parallel tempering on the device (parallel_tempering.cu:93-352) */
+/* Every sample gets NT temperatures x nrep_per_temp replicas (its nrep must
+ * equal NT*nrep_per_temp).  beta_sched[NT], index 0 hottest.  The
+ * exchange draws from a drand48 stream seeded like srand48(seed+5000). */
+int  pspin_pt_init(pspin_state* s, int NT, int nrep_per_temp, const double* beta_sched,
+                   int pt_freq);
+/* Runs nsweeps sweeps; after every sweep whose 1-based index is a multiple
+ * of pt_freq, proposes the NT-1 adjacent exchanges per replica column. */
+int  pspin_pt_run(pspin_state* s, int nsweeps);
+/* perm[NT*nrep_per_temp] (logical t*nrep+r -> physical replica) and the
+ * cumulative exchange counters [NT-1] of one sample. */
+int  pspin_pt_get(pspin_state* s, int sample, int32_t* perm, int64_t* ex_acc, int64_t* ex_prop);
+int  pspin_pt_sweeps_done(pspin_state* s, int64_t* sweeps);
+
+/* ---- per-move trace (tests) ------------------------------------------ */
+int  pspin_trace_get(pspin_state* s, pspin_move_record* out, int max_records, int* n_records);
+
+/* ---- stand-alone kernels the reference's unit tests exercise --------- */
+/* disorder.cu:153-183 on the GPU: first-pass-wins channel mask over C(N,4). */
+int  pspin_fmc_mask(int N, const double* omega, double gamma, uint8_t* mask_out,
+                    int64_t* n_active);
+/* test_quartet_index.cu:56-74 on the GPU: decode -> order -> re-encode for
+ * every q < C(N,4); *n_fail counts mismatches. */
+int  pspin_quartet_roundtrip(int N, int64_t* n_fail);
+
+/* ---- measurement (no reference counterpart) --------------------------- */
+/* The CUDA stream (cudaStream_t) all of this handle's work runs on. */
+void* pspin_stream(pspin_state* s);
+/* When on, every sweep-kernel launch is bracketed by CUDA events on the
+ * handle's stream; pspin_get_profile sums their durations since the last
+ * call and also reports how many kernels of this library were launched. */
+int  pspin_set_profiling(pspin_state* s, int on);
+int  pspin_get_profile(pspin_state* s, double* sweep_kernel_ms, int64_t* sweep_launches,
+                       int64_t* kernel_launches);
+/* FP32 FMA throughput of the current device (TFLOP/s), measured by a
+ * register-resident FMA loop over all SMs: the roofline denominator of the
+ * FP32 sweep. */
+int  pspin_fp32_peak(double* tflops);
+
+/* ---- errors ---------------------------------------------------------- */
+const char* pspin_last_error(void);
+const char* pspin_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSPIN_H */

@@ -1,0 +1,61 @@
+"""The C ABI library: loads without a GPU, exports every symbol that
+include/pspin.h declares, and its host-only entry points (config defaults and
+the reference's argv parser, config.h:28-46 and config.cu:6-70) behave like
+the reference's.  No compute call is made here."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "pspin.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(pspin_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol(ps):
+    lib = ps.load_library()
+    names = declared_symbols()
+    assert len(names) >= 29
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_default_config_matches_reference(ps):
+    c = ps.default_config()
+    assert (c.N, c.nrep, c.T, c.J, c.J0, c.alpha, c.alpha0) == (64, 1, 1.0, 2.0, 0.0, 0.5, 0.5)
+    assert (c.mc_iterations, c.seed, c.save_freq, c.verbose, c.label, c.dev, c.fmc_mode, c.gamma) == \
+        (10000, 42, 100, 0, -1, -1, 0, 0.0)
+    assert ctypes.sizeof(ps.SimConfig) == 96      # SimConfig is 96 bytes
+
+
+def test_parse_args(ps):
+    c = ps.parse_args(["x", "-N", "32", "-nrep", "4", "-fmc", "2", "-seed", "17", "-verbose"])
+    assert (c.N, c.nrep, c.fmc_mode, c.seed, c.verbose) == (32, 4, 2, 17, 1)
+    assert c.gamma == 1.0 / 62.0                     # config.cu:61-67
+    c = ps.parse_args(["x", "-fmc", "1", "-verbose", "2", "-gamma", "0.5"])
+    assert (c.fmc_mode, c.gamma, c.verbose) == (1, 0.5, 2)
+    c = ps.parse_args(["x", "-fmc", "1"])
+    assert c.gamma == 0.0
+    with pytest.raises(ps.PspinError) as e:
+        ps.parse_args(["x", "-bogus"])
+    assert "Unknown argument: -bogus" in str(e.value)
+    with pytest.raises(ps.PspinError) as e:
+        ps.parse_args(["x", "-N", "3"])
+    assert "N must be >= 4" in str(e.value)
+
+
+def test_version_and_error_string(ps):
+    lib = ps.load_library()
+    assert b"sm_100a" in lib.pspin_version()
+    assert isinstance(lib.pspin_last_error(), bytes)
+
+
+def test_bad_arguments_return_codes(ps):
+    lib = ps.load_library()
+    assert lib.pspin_create_batch(None, 0, 0, None, None) == 1
+    assert lib.pspin_destroy(None) == 0
