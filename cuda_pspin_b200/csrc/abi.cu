@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <chrono>
 #include <unordered_map>
 #include <vector>
 
@@ -45,6 +46,13 @@ static int fail(int code, const char* fmt, ...) {
     g_err = buf;
     return code;
 }
+
+namespace pspin {
+int report_error(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+}  // namespace pspin
 
 #define CK(call)                                                                                     \
     do {                                                                                             \
@@ -686,6 +694,12 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     std::vector<std::vector<float2>> spins(n);
     std::vector<std::vector<double>> targets(n);
     std::vector<std::vector<uint64_t>> keys(n);
+    const bool timing = std::getenv("PSPIN_SETUP_TIMING") != nullptr;
+    auto clk = [] { return std::chrono::steady_clock::now(); };
+    auto secs = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+        return std::chrono::duration<double>(b - a).count();
+    };
+    const auto t_p1 = clk();
     // phase 1 (device, in sample order): cuRAND streams, FMC masks, survivor
     // counts, coupling rescale; host copies of what the layout needs
     std::vector<std::vector<QuartetRec>> qsv(n);
@@ -714,8 +728,18 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
             double* d = nullptr;
             rc = dalloc(&d, nrm.size());
             if (rc != PSPIN_OK) return bail(rc);
-            for (int r = 0; r < R && rc == PSPIN_OK; r++)
-                rc = curand_normals(keys[k][r], 2 * (size_t)N, d + 2 * (size_t)N * r, s->st);
+            // one generator, re-seeded with its offset reset for every
+            // replica: the stream of a fresh generator with that seed
+            Curand c;
+            curandStatus_t cs = curandCreateGenerator(&c.g, CURAND_RNG_PSEUDO_PHILOX4_32_10);
+            if (cs == CURAND_STATUS_SUCCESS) cs = curandSetStream(c.g, s->st);
+            for (int r = 0; r < R && cs == CURAND_STATUS_SUCCESS; r++) {
+                cs = curandSetPseudoRandomGeneratorSeed(c.g, keys[k][r]);
+                if (cs == CURAND_STATUS_SUCCESS) cs = curandSetGeneratorOffset(c.g, 0);
+                if (cs == CURAND_STATUS_SUCCESS)
+                    cs = curandGenerateNormalDouble(c.g, d + 2 * (size_t)N * r, 2 * (size_t)N, 0.0, 1.0);
+            }
+            if (cs != CURAND_STATUS_SUCCESS) rc = fail(PSPIN_ERR_CURAND, "spin init cuRAND error %d", (int)cs);
             if (rc == PSPIN_OK) {
                 cudaError_t e = cudaMemcpyAsync(nrm.data(), d, nrm.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
@@ -725,6 +749,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
             if (rc != PSPIN_OK) return bail(rc);
         }
     }
+    const auto t_p2 = clk();
     // phase 2 (host, samples in parallel): normalisation, quartet lists,
     // per-site sweep lists, FP64 quartet tables
 #pragma omp parallel for schedule(dynamic, 1)
@@ -751,6 +776,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         h.site_entries = (int64_t)lists[k].entries.size();
     }
 
+    const auto t_p3 = clk();
     // ---- concatenate and upload
     int64_t ent_total = 0, split_total = 0, q_total = 0, g2_total = 0, spin_off = 0, rep_off = 0, chunk_total = 0;
     s->sd.resize(n);
@@ -871,6 +897,9 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         cudaError_t e = cudaStreamSynchronize(s->st);
         if (e != cudaSuccess) return bail(fail(PSPIN_ERR_CUDA, "init: %s", cudaGetErrorString(e)));
     }
+    if (timing)
+        fprintf(stderr, "[pspin set-up] device phase %.3f s, host layout %.3f s, upload+energies %.3f s\n",
+                secs(t_p1, t_p2), secs(t_p2, t_p3), secs(t_p3, clk()));
     *out = s;
     return PSPIN_OK;
 }
