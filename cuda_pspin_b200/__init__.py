@@ -105,6 +105,7 @@ def load_library() -> ctypes.CDLL:
         "pspin_trace_get": (ctypes.c_int, [vp, vp, ctypes.c_int, vp]),
         "pspin_fmc_mask": (ctypes.c_int, [ctypes.c_int, vp, ctypes.c_double, vp, vp]),
         "pspin_quartet_roundtrip": (ctypes.c_int, [ctypes.c_int, vp]),
+        "pspin_fmc_survivors_static": (ctypes.c_int, [ctypes.c_int, vp, ctypes.c_double, vp, vp]),
         "pspin_stream": (vp, [vp]),
         "pspin_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
         "pspin_get_profile": (ctypes.c_int, [vp, vp, vp, vp]),

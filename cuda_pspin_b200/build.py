@@ -24,7 +24,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "layout.cpp"]
+LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "noalloc.cu", "layout.cpp"]
 DRIVERS = {
     "pspin_pt": ["drivers/pt_main.cpp"],
     "pspin_pt_sparse": ["drivers/pt_sparse_main.cpp"],

@@ -163,6 +163,20 @@ int  pspin_fmc_mask(int N, const double* omega, double gamma, uint8_t* mask_out,
  * every q < C(N,4); *n_fail counts mismatches. */
 int  pspin_quartet_roundtrip(int N, int64_t* n_fail);
 
+/* ---- allocation-free survivor count (no counterpart in the reference) ---
+ * For callers that cannot call cudaMalloc (work recorded while a stream is
+ * captured, hosts whose own pool owns all device memory, plugins handed
+ * only device pointers): counts the quartet-channel pairs that pass the FMC
+ * filter, like pspin_fmc_mask's n_active, without allocating.  omega[N] and
+ * counts[4] (total, channel 0, 1, 2) are device pointers; stream is a
+ * cudaStream_t (NULL: the default stream); the call is asynchronous on it.
+ * Intermediate per-row counts live in one static device array sized for
+ * N <= 1024 (larger N returns PSPIN_ERR_ARG).  The first call on a device
+ * looks up that array's address and should come before any stream capture.
+ * Calls that overlap on the GPU share the array and race. */
+int  pspin_fmc_survivors_static(int N, const double* omega, double gamma, int64_t* counts,
+                                void* stream);
+
 /* ---- measurement (no reference counterpart) --------------------------- */
 /* The CUDA stream (cudaStream_t) all of this handle's work runs on. */
 void* pspin_stream(pspin_state* s);
