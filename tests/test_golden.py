@@ -73,6 +73,27 @@ def test_oracle_reproduces_reference(orc, name):
     np.testing.assert_allclose(ref.energies, g["energies"], rtol=0, atol=1e-13 * N)
 
 
+def test_oracle_sparse_selection_n512(orc):
+    """mc_sparse_init's selection at N=512, comb, gamma=1: the oracle walks
+    the 2.83e9 quartets in q order without storing them and must pick the
+    reference's 512 (quartet, channel) pairs out of its 33,130,110 survivors."""
+    import ctypes
+    g = load("sparse_n512_fmc1_s42")
+    N = 512
+    w = orc.omega(N, 1, 42)
+    enc = np.zeros(N, np.int64)
+    nnz = ctypes.c_int64()
+    assert orc.lib().orc_sparse_select(N, orc.P(w), 1.0, 1, 42, N, orc.P(enc), ctypes.byref(nnz)) == 0
+    assert nnz.value == int(g["info"][5]) == 33130110
+    L = orc.lib()
+    i, j, k, l = (ctypes.c_int() for _ in range(4))
+    got = []
+    for e in enc:
+        L.orc_decode_quartet(int(e) // 3, ctypes.byref(i), ctypes.byref(j), ctypes.byref(k), ctypes.byref(l))
+        got.append((i.value, j.value, k.value, l.value, int(e) % 3))
+    assert np.array_equal(np.array(got, np.int32), g["quartets"])
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", NAMES)
 def test_engine_reproduces_reference(ps, orc, name):

@@ -1,0 +1,58 @@
+"""Multi-rank path of bench.py on CPU with gloo (world size 2).
+
+The path shards by independent disorder samples: every rank runs its own
+samples (weak scaling) and the only cross-rank operations are a barrier and
+the max of the timings.  Checked here: the shards are disjoint and complete,
+and the MAX reduction bench.py applies gives the slowest rank's time.
+"""
+import os
+import socket
+
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    Ns, seeds = bench.workload(256, rank)
+    gathered = [None] * world
+    dist.all_gather_object(gathered, (Ns, seeds))
+    t = torch.tensor([10.0 + rank])
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    if rank == 0:
+        q.put((gathered, float(t.item())))
+    dist.destroy_process_group()
+
+
+def test_sample_sharding_and_max_timing():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    gathered, tmax = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (N0, s0), (N1, s1) = gathered
+    assert N0 == N1                          # same N mix on every rank
+    assert not set(s0) & set(s1)             # disjoint disorder samples
+    assert sorted(s0 + s1) == list(range(1000, 1000 + 512))
+    assert tmax == 11.0                      # the slowest rank's time
+    assert sorted(set(N0)) == [24, 32, 48, 64]
