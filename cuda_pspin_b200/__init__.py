@@ -51,7 +51,7 @@ class Options(ctypes.Structure):
     _fields_ = [("init_exact", ctypes.c_int), ("resync_every", ctypes.c_int),
                 ("warps_per_unit", ctypes.c_int), ("trace_sample", ctypes.c_int),
                 ("trace_replica", ctypes.c_int), ("trace_capacity", ctypes.c_int),
-                ("quiet", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+                ("quiet", ctypes.c_int), ("generic_lists", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 
 class Info(ctypes.Structure):
@@ -150,8 +150,10 @@ def parse_args(argv: list[str]) -> SimConfig:
 
 
 def make_options(init_exact: bool = False, resync_every: int = 0, warps_per_unit: int = 0,
-                 trace: tuple[int, int, int] | None = None, quiet: bool = True) -> Options:
+                 trace: tuple[int, int, int] | None = None, quiet: bool = True,
+                 generic_lists: bool = False) -> Options:
     o = Options()
+    o.generic_lists = int(generic_lists)
     o.init_exact = int(init_exact)
     o.resync_every = resync_every
     o.warps_per_unit = warps_per_unit

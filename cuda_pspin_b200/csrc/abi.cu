@@ -99,6 +99,7 @@ struct SampleHost {
     std::vector<double> sqg;
     int64_t site_entries = 0;
     int64_t g4_off = -1;             // dense: into d_g4re / d_mask
+    int fc_tiles = 0;                // site lists are fully connected tiles
     int64_t nq_dense = 0;
 };
 
@@ -756,11 +757,18 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     for (int k = 0; k < n; k++) {
         SampleHost& h = s->hs[k];
         const int N = h.N, R = h.R;
+        bool fc = false;
         if (variant == PSPIN_DENSE) {
             dense_quartets(N, g4h[k].data(), maskh[k].data(), qsv[k]);
+            // fully connected tiles when every quartet is active in channel 0
+            fc = !s->opt.generic_lists && h.cfg.fmc_mode == 0 && (int64_t)qsv[k].size() == C4(N);
+            for (const QuartetRec& r : qsv[k])
+                if (!fc || r.ch != 0) { fc = false; break; }
+            if (fc) build_site_tiles_fc(N, h.g2re.data(), h.h2_active, g4h[k].data(), lists[k]);
             std::vector<double>().swap(g4h[k]);
             std::vector<uint8_t>().swap(maskh[k]);
         }
+        h.fc_tiles = fc ? 1 : 0;
         targets[k].resize(R);
         spins[k].resize((size_t)N * R);
         for (int r = 0; r < R; r++) {
@@ -770,7 +778,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
                 spins[k][(size_t)i * R + r] = make_float2((float)sp[2 * i], (float)sp[2 * i + 1]);
         }
         std::vector<double>().swap(nrmv[k]);
-        build_site_lists(N, h.g2re.data(), h.h2_active, qsv[k], lists[k]);
+        if (!fc) build_site_lists(N, h.g2re.data(), h.h2_active, qsv[k], lists[k]);
         build_q64(qsv[k], q64[k]);
         std::vector<QuartetRec>().swap(qsv[k]);
         h.site_entries = (int64_t)lists[k].entries.size();
@@ -787,6 +795,8 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         d.R = h.R;
         d.h2_active = h.h2_active;
         d.variant = variant;
+        d.fc_tiles = h.fc_tiles;
+        d.pad0 = 0;
         d.spin_off = spin_off;
         d.rep_off = rep_off;
         d.split_off = split_total;

@@ -30,6 +30,16 @@
 // local field h_m = sum over m's quartets of g a_p conj(a_o1 a_o2) gives
 // every energy change of site m alone as -Re[da_m h_m].  2-body terms fold
 // in with p = o1 = N, a virtual site whose amplitude is 1.
+//
+// Fully connected tiles.  When every quartet is active in channel 0, a
+// quartet enters site m's field as g a_p conj(a_outer) conj(a_inner) with a
+// contiguous range of inner sites shared by every partner p of one outer
+// site: if m is among the two smallest sites of the quartet, outer = o1 > m,
+// p < o1 and inner in (o1, N); otherwise outer = o2 < m, p > o2 and inner in
+// [0, o2).  A tile is a 16-byte header {outer | lo<<16, hi, p0 | p1<<16,
+// p2 | p3<<16} and hi-lo rows of 4 couplings (one per partner; padding
+// partners are the virtual site with zero couplings), so one gathered
+// a_inner feeds 8 FFMA.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -39,7 +49,7 @@ namespace pspin {
 constexpr int kSplit = 32;        // parts per site list (warps per unit divide it)
 constexpr int kGroupMax = 32;     // max data entries after one header
 constexpr int kStage = 256;       // max entries per TMA chunk (2 KB)
-constexpr int kStages = 4;        // chunks in flight per warp
+constexpr int kStages = 3;        // chunks in flight per warp
 constexpr int kRepBlock = 32;     // replicas per unit (one per lane)
 
 struct SampleDev {
@@ -47,6 +57,8 @@ struct SampleDev {
     int R;                 // replicas of this sample
     int h2_active;
     int variant;           // 0 sphere (dense), 1 smoothed cube (sparse)
+    int fc_tiles;          // 1: site lists are fully connected tiles (see below)
+    int pad0;
     int64_t spin_off;      // float2 index of site 0, replica 0
     int64_t rep_off;       // index into the per-replica arrays
     int64_t split_off;     // index into site chunks (N*33 entries)

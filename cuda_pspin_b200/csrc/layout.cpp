@@ -38,6 +38,41 @@ struct Rec {
     float g;
 };
 
+// Cuts one site's records (groups or tiles, [begin, end) in int2 units of
+// `site`) into 32 parts of nearly equal size and packs every part in TMA
+// chunks of whole records, <= kStage entries, padded to an even length.
+static void pack_site(const std::vector<int2>& site, const std::vector<std::pair<int64_t, int64_t>>& groups, int m,
+                      SiteLists& out) {
+    const int64_t total = (int64_t)site.size();
+    std::vector<size_t> part_first(kSplit + 1, groups.size());
+    part_first[0] = 0;
+    size_t g = 0;
+    for (int part = 1; part < kSplit; part++) {
+        const int64_t target = (total * part) / kSplit;
+        while (g < groups.size() && groups[g].first < target) g++;
+        part_first[part] = g;
+    }
+    int* sc = &out.site_chunks[(size_t)m * (kSplit + 1)];
+    for (int part = 0; part < kSplit; part++) {
+        sc[part] = (int)out.chunk_start.size();
+        size_t gi = part_first[part];
+        const size_t ge = std::max(part_first[part], part_first[part + 1]);
+        while (gi < ge) {
+            out.chunk_start.push_back((int64_t)out.entries.size());
+            int64_t len = 0;
+            while (gi < ge) {
+                const int64_t gl = groups[gi].second - groups[gi].first;
+                if (len > 0 && len + gl + 1 > kStage) break;
+                out.entries.insert(out.entries.end(), site.begin() + groups[gi].first, site.begin() + groups[gi].second);
+                len += gl;
+                gi++;
+            }
+            if (len & 1) out.entries.push_back(make_int2(0, 0));
+        }
+    }
+    sc[kSplit] = (int)out.chunk_start.size();
+}
+
 void build_site_lists(int N, const double* g2re, int h2_active, const std::vector<QuartetRec>& qs,
                       SiteLists& out) {
     std::vector<std::vector<Rec>> per(N);
@@ -90,39 +125,80 @@ void build_site_lists(int N, const double* g2re, int h2_active, const std::vecto
             groups.push_back({gb, (int64_t)site.size()});
             t = e;
         }
-        // 32 parts of nearly equal size, cut at group starts
-        const int64_t total = (int64_t)site.size();
-        std::vector<size_t> part_first(kSplit + 1, groups.size());
-        part_first[0] = 0;
-        size_t g = 0;
-        for (int part = 1; part < kSplit; part++) {
-            const int64_t target = (total * part) / kSplit;
-            while (g < groups.size() && groups[g].first < target) g++;
-            part_first[part] = g;
-        }
-        // every part packed in chunks of whole groups, <= kStage entries,
-        // padded with an empty group to an even length (16-byte granules)
-        int* sc = &out.site_chunks[(size_t)m * (kSplit + 1)];
-        for (int part = 0; part < kSplit; part++) {
-            sc[part] = (int)out.chunk_start.size();
-            size_t gi = part_first[part];
-            const size_t ge = std::max(part_first[part], part_first[part + 1]);
-            while (gi < ge) {
-                const int64_t cb = (int64_t)out.entries.size();
-                out.chunk_start.push_back(cb);
-                int64_t len = 0;
-                while (gi < ge) {
-                    const int64_t gl = groups[gi].second - groups[gi].first;
-                    if (len > 0 && len + gl + 1 > kStage) break;
-                    out.entries.insert(out.entries.end(), site.begin() + groups[gi].first,
-                                       site.begin() + groups[gi].second);
-                    len += gl;
-                    gi++;
-                }
-                if (len & 1) out.entries.push_back(make_int2(0, 0));
+        pack_site(site, groups, m, out);
+    }
+}
+
+static inline int64_t encode_sorted(int a, int b, int c, int d) {
+    int v[4] = {a, b, c, d};
+    std::sort(v, v + 4);
+    return (int64_t)v[3] * (v[3] - 1) * (v[3] - 2) * (v[3] - 3) / 24 + (int64_t)v[2] * (v[2] - 1) * (v[2] - 2) / 6 +
+           (int64_t)v[1] * (v[1] - 1) / 2 + v[0];
+}
+
+static inline int fbits(float f) {
+    int b;
+    std::memcpy(&b, &f, sizeof(int));
+    return b;
+}
+
+void build_site_tiles_fc(int N, const double* g2re, int h2_active, const double* g4re, SiteLists& out) {
+    out.entries.clear();
+    out.chunk_start.clear();
+    out.site_chunks.assign((size_t)N * (kSplit + 1), 0);
+    std::vector<int2> site;
+    std::vector<std::pair<int64_t, int64_t>> tiles;
+    std::vector<int> partners;
+    for (int m = 0; m < N; m++) {
+        site.clear();
+        tiles.clear();
+        // one tile: header + (hi-lo) rows of 4 couplings; coef(k, t) for partner k, inner t
+        auto emit = [&](int outer, int lo, int hi, const int* p, auto coef) {
+            const int64_t b = (int64_t)site.size();
+            site.push_back(make_int2(outer | (lo << 16), hi));
+            site.push_back(make_int2(p[0] | (p[1] << 16), p[2] | (p[3] << 16)));
+            for (int t = lo; t < hi; t++) {
+                site.push_back(make_int2(fbits(coef(0, t)), fbits(coef(1, t))));
+                site.push_back(make_int2(fbits(coef(2, t)), fbits(coef(3, t))));
+            }
+            tiles.push_back({b, (int64_t)site.size()});
+        };
+        if (h2_active) {
+            const int pv[4] = {N, N, N, N};
+            for (int lo = 0; lo < N; lo += kGroupMax) {
+                const int hi = std::min(N, lo + kGroupMax);
+                emit(N, lo, hi, pv, [&](int k, int t) {
+                    return (k == 0 && t != m) ? (float)g2re[(size_t)m * N + t] : 0.0f;
+                });
             }
         }
-        sc[kSplit] = (int)out.chunk_start.size();
+        // m among the two smallest: outer o1 > m, partners p < o1, inner o2 in (o1, N)
+        // m among the two largest: outer o2 < m, partners p > o2, inner o1 in [0, o2)
+        for (int side = 0; side < 2; side++) {
+            const int o_begin = side == 0 ? m + 1 : 0, o_end = side == 0 ? N : m;
+            for (int outer = o_begin; outer < o_end; outer++) {
+                const int ilo = side == 0 ? outer + 1 : 0, ihi = side == 0 ? N : outer;
+                if (ilo >= ihi) continue;
+                partners.clear();
+                if (side == 0) { for (int p = 0; p < outer; p++) if (p != m) partners.push_back(p); }
+                else { for (int p = outer + 1; p < N; p++) if (p != m) partners.push_back(p); }
+                for (size_t pb = 0; pb < partners.size(); pb += 4) {
+                    int pv[4];
+                    bool real[4];
+                    for (int k = 0; k < 4; k++) {
+                        real[k] = pb + k < partners.size();
+                        pv[k] = real[k] ? partners[pb + k] : N;
+                    }
+                    for (int lo = ilo; lo < ihi; lo += kGroupMax) {
+                        const int hi = std::min(ihi, lo + kGroupMax);
+                        emit(outer, lo, hi, pv, [&](int k, int t) {
+                            return real[k] ? (float)g4re[encode_sorted(m, pv[k], outer, t)] : 0.0f;
+                        });
+                    }
+                }
+            }
+        }
+        pack_site(site, tiles, m, out);
     }
 }
 

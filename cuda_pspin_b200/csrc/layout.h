@@ -20,6 +20,8 @@ struct SiteLists {
 
 void build_site_lists(int N, const double* g2re, int h2_active, const std::vector<QuartetRec>& qs,
                       SiteLists& out);
+// fully connected tiles from the dense g4 (channel 0 everywhere) and g2
+void build_site_tiles_fc(int N, const double* g2re, int h2_active, const double* g4re, SiteLists& out);
 void build_q64(const std::vector<QuartetRec>& qs, std::vector<Q64>& out);
 // every active (q, ch) of a dense mask in q order
 void dense_quartets(int N, const double* g4re, const uint8_t* mask, std::vector<QuartetRec>& out);

@@ -187,8 +187,49 @@ __device__ __forceinline__ void accumulate_chunk(const int2* __restrict__ R, int
     }
 }
 
+// Field contribution of the fully connected tiles in one staged chunk
+// (16-byte records: header, then rows of 4 couplings).  One gathered
+// a_inner feeds four partners: 8 FFMA per shared-memory gather.
+__device__ __forceinline__ void accumulate_tiles(const int2* __restrict__ R2, int n,
+                                                 const float2* __restrict__ sp, int lane,
+                                                 float& hx, float& hy) {
+    const int4* __restrict__ R = reinterpret_cast<const int4*>(R2);
+    const int n16 = n >> 1;
+    int e = 0;
+    while (e < n16) {
+        const int4 hd = R[e];
+        const int outer = hd.x & 0xFFFF, lo = hd.x >> 16, hi = hd.y;
+        const float2 ao = sp[outer * kRepBlock + lane];
+        float y0x = 0.f, y0y = 0.f, y1x = 0.f, y1y = 0.f, y2x = 0.f, y2y = 0.f, y3x = 0.f, y3y = 0.f;
+        const float4* __restrict__ C = reinterpret_cast<const float4*>(R + e + 1);
+        const float2* __restrict__ A = sp + lo * kRepBlock + lane;
+        const int len = hi - lo;
+#pragma unroll 2
+        for (int t = 0; t < len; t++) {
+            const float4 c = C[t];
+            const float2 a = A[t * kRepBlock];
+            y0x = fmaf(c.x, a.x, y0x); y0y = fmaf(-c.x, a.y, y0y);
+            y1x = fmaf(c.y, a.x, y1x); y1y = fmaf(-c.y, a.y, y1y);
+            y2x = fmaf(c.z, a.x, y2x); y2y = fmaf(-c.z, a.y, y2y);
+            y3x = fmaf(c.w, a.x, y3x); y3y = fmaf(-c.w, a.y, y3y);
+        }
+        // h += sum_k a_pk conj(a_outer) Y_k
+        const int pk[4] = {hd.z & 0xFFFF, hd.z >> 16, hd.w & 0xFFFF, hd.w >> 16};
+        const float yx[4] = {y0x, y1x, y2x, y3x}, yy[4] = {y0y, y1y, y2y, y3y};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float2 ap = sp[pk[k] * kRepBlock + lane];
+            const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
+            const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
+            hx = fmaf(px, yx[k], fmaf(-py, yy[k], hx));
+            hy = fmaf(px, yy[k], fmaf(py, yx[k], hy));
+        }
+        e += 1 + len;
+    }
+}
+
 template <int VARIANT>
-__global__ void __launch_bounds__(256, 2) sweep_kernel(const SweepParams P) {
+__global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Unit U = P.units[blockIdx.x];
     const SampleDev S = P.samples[U.sample];
@@ -297,7 +338,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(const SweepParams P) {
                 const uint32_t slot = consumed % kStages;
                 if (ok) ok = mbar_wait(bars + slot, (consumed / kStages) & 1u, P.status);
                 const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
-                accumulate_chunk(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
+                if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
+                else accumulate_chunk(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
                 consumed++;
                 __syncwarp();
                 if (lane == 0) fence_async_shared();

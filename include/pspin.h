@@ -78,7 +78,9 @@ typedef struct pspin_options {
     int trace_replica;   /*   ... physical replica; <0 disables tracing */
     int trace_capacity;  /*   ... number of move records kept */
     int quiet;           /* suppress the reference's stdout lines */
-    int reserved[7];
+    int generic_lists;   /* 1: per-entry site lists for every sample; 0 (default):
+                            fully connected dense samples use blocked tiles */
+    int reserved[6];
 } pspin_options;
 
 typedef struct pspin_info {

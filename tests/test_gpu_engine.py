@@ -107,11 +107,13 @@ def test_sparse_init_matches_oracle(ps, orc, kw):
 
 
 # ---- per-move dE against the FP64 oracle ----------------------------------------------
-def _trace_run(ps, orc, kw, variant, nsweeps=12, rep=1, T=0.7):
+def _trace_run(ps, orc, kw, variant, nsweeps=12, rep=1, T=0.7, generic=False):
     c, oc = cfg_pair(ps, orc, **kw)
+    if variant == ps.PSPIN_DENSE and c.N > 32:
+        nsweeps = 3        # the CPU replay costs two full C(N,4) energies per move
     ref = orc.DenseInit(oc) if variant == ps.PSPIN_DENSE else orc.SparseInit(oc)
     cap = nsweeps * (c.N // 2)
-    with ps.Engine(c, variant, ps.make_options(trace=(0, rep, cap), resync_every=-1)) as eng:
+    with ps.Engine(c, variant, ps.make_options(trace=(0, rep, cap), resync_every=-1, generic_lists=generic)) as eng:
         s0 = eng.get_spins()[0][rep].copy()
         eng.fill_betas(1.0 / T)
         eng.sweep(nsweeps)
@@ -127,9 +129,14 @@ def _trace_run(ps, orc, kw, variant, nsweeps=12, rep=1, T=0.7):
                                 dict(N=12, nrep=33, fmc_mode=2, seed=7),
                                 dict(N=16, nrep=8, fmc_mode=0, seed=5, J0=0.5),
                                 dict(N=20, nrep=4, fmc_mode=1, seed=3, gamma=2.0),
-                                dict(N=32, nrep=2, fmc_mode=2, seed=42, gamma=0.1)])
-def test_dense_per_move_dE(ps, orc, kw):
-    worst, tr, s0, s1, nacc, ref = _trace_run(ps, orc, kw, ps.PSPIN_DENSE)
+                                dict(N=32, nrep=2, fmc_mode=2, seed=42, gamma=0.1),
+                                dict(N=48, nrep=4, fmc_mode=0, seed=21),
+                                dict(N=64, nrep=3, fmc_mode=0, seed=22)])
+@pytest.mark.parametrize("generic", [False, True])
+def test_dense_per_move_dE(ps, orc, kw, generic):
+    """Fully connected samples run on the blocked tiles by default and on the
+    per-entry lists with generic_lists; both must meet the bound."""
+    worst, tr, s0, s1, nacc, ref = _trace_run(ps, orc, kw, ps.PSPIN_DENSE, generic=generic)
     assert worst <= 1e-5, worst
     assert 0 < tr["accepted"].sum() == nacc
     # replaying accepted moves reproduces the final amplitudes exactly
