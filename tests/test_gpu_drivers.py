@@ -1,0 +1,113 @@
+"""The drop-in drivers against the reference's own programs.
+
+pspin_pt / pspin_pt_sparse / pspin_mc take the reference's flags and write
+its files.  Each is run next to the reference's binary (rebuilt for sm_100a
+from its sources into oracle/_ref/) with the same flags in separate working
+directories:
+  * files fixed by the disorder and the flags (params.txt, temperatures.txt,
+    frequencies.txt, quartets.txt, the time.txt header) are byte-identical;
+  * files with sampled values (energy_accept.txt, exchanges.txt,
+    energy_split.txt, configs.bin) have the same headers, rows, columns and
+    sizes;
+  * the reference's analysis_pt reads the engine's output and completes.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "cuda_pspin_b200", "bin")
+REF = os.path.join(ROOT, "oracle", "_ref")
+
+
+def run(cmd, cwd):
+    p = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+    return p
+
+
+def the_dir(base):
+    data = os.path.join(base, "data")
+    d = [x for x in os.listdir(data)]
+    assert len(d) == 1, d
+    return os.path.join(data, d[0])
+
+
+def table(path):
+    lines = open(path).read().splitlines()
+    rows = [ln.split("\t") for ln in lines[1:]]
+    return lines[0], rows
+
+
+PT_FLAGS = ["-N", "12", "-Tmax", "1.6", "-Tmin", "0.2", "-NT", "4", "-log_temp", "-nrep", "2", "-iter", "64",
+            "-pt_freq", "1", "-save_freq", "8", "-seed", "42", "-fmc", "2", "-gamma", "0.3", "-label", "3"]
+
+
+@pytest.mark.parametrize("variant", ["dense", "sparse"])
+def test_pt_driver_matches_reference_files(tmp_path, variant):
+    sparse = variant == "sparse"
+    flags = list(PT_FLAGS)
+    if sparse:
+        flags = [f if f != "12" else "16" for f in flags]
+    ours, ref = tmp_path / "ours", tmp_path / "ref"
+    ours.mkdir()
+    ref.mkdir()
+    run([os.path.join(BIN, "pspin_pt_sparse" if sparse else "pspin_pt"), *flags], ours)
+    run([os.path.join(REF, "parallel_tempering_sparse" if sparse else "parallel_tempering"), *flags], ref)
+    d_o, d_r = the_dir(ours), the_dir(ref)
+    assert os.path.basename(d_o) == os.path.basename(d_r)         # make_run_dir naming
+    files_r = sorted(os.listdir(d_r))
+    assert sorted(os.listdir(d_o)) == files_r
+    same = ["params.txt", "temperatures.txt", "frequencies.txt"] + (["quartets.txt"] if sparse else [])
+    for f in same:
+        assert open(os.path.join(d_o, f)).read() == open(os.path.join(d_r, f)).read(), f
+    assert open(os.path.join(d_o, "time.txt")).readline() == open(os.path.join(d_r, "time.txt")).readline()
+    for f in ["energy_accept.txt", "exchanges.txt", "energy_split.txt"]:
+        h_o, r_o = table(os.path.join(d_o, f))
+        h_r, r_r = table(os.path.join(d_r, f))
+        assert h_o == h_r, f
+        assert len(r_o) == len(r_r), f
+        assert [len(x) for x in r_o] == [len(x) for x in r_r], f
+        assert [x[:3] for x in r_o] == [x[:3] for x in r_r], f      # sweep, Tidx, T columns
+    assert os.path.getsize(os.path.join(d_o, "configs.bin")) == os.path.getsize(os.path.join(d_r, "configs.bin"))
+    # exchange counts per window: same number of proposals
+    _, ex_o = table(os.path.join(d_o, "exchanges.txt"))
+    _, ex_r = table(os.path.join(d_r, "exchanges.txt"))
+    assert [x[5] for x in ex_o] == [x[5] for x in ex_r]
+
+
+def test_analysis_pt_reads_engine_output(tmp_path):
+    flags = ["-N", "12", "-Tmax", "1.6", "-Tmin", "0.3", "-NT", "4", "-log_temp", "-nrep", "2", "-iter", "256",
+             "-pt_freq", "1", "-save_freq", "16", "-seed", "7", "-label", "0", "-batch", "3"]
+    run([os.path.join(BIN, "pspin_pt"), *flags], tmp_path)
+    assert len(os.listdir(tmp_path / "data")) == 3                    # -batch 3: three sample dirs
+    p = run([os.path.join(REF, "analysis_pt"), "-N", "12", "-NT", "4", "-nrep", "2", "--log-temp"], tmp_path)
+    assert "samples" in p.stdout
+    out = tmp_path / "analysis"
+    produced = [f for _, _, fs in os.walk(out) for f in fs]
+    assert len(produced) > 0, p.stdout[-2000:]
+
+
+def test_mc_driver_matches_reference_files(tmp_path):
+    flags = ["-N", "12", "-nrep", "3", "-T", "0.8", "-iter", "40", "-save_freq", "10", "-seed", "5", "-label", "1"]
+    ours, ref = tmp_path / "ours", tmp_path / "ref"
+    ours.mkdir()
+    ref.mkdir()
+    run([os.path.join(BIN, "pspin_mc"), *flags], ours)
+    run([os.path.join(REF, "pspin24"), *flags], ref)
+    d_o, d_r = the_dir(ours), the_dir(ref)
+    assert os.path.basename(d_o) == os.path.basename(d_r)
+    h_o, r_o = table(os.path.join(d_o, "energy_accept.txt"))
+    h_r, r_r = table(os.path.join(d_r, "energy_accept.txt"))
+    assert h_o == h_r and len(r_o) == len(r_r) and [x[0] for x in r_o] == [x[0] for x in r_r]
+    assert sorted(os.listdir(os.path.join(d_o, "configs"))) == sorted(os.listdir(os.path.join(d_r, "configs")))
+    assert open(os.path.join(d_o, "time_per_iter.txt")).readline() == \
+        open(os.path.join(d_r, "time_per_iter.txt")).readline()
+    # the first saved energies agree at the start of the run only statistically;
+    # check they are finite and the acceptance is a rate
+    vals = np.array([[float(v) for v in x[1:]] for x in r_o])
+    assert np.all(np.isfinite(vals)) and np.all((vals[:, 1::2] >= 0) & (vals[:, 1::2] <= 1))
