@@ -25,6 +25,8 @@ BIN_DIR = os.path.join(_HERE, "bin")
 
 PSPIN_DENSE = 0
 PSPIN_SPARSE = 1
+FIELDS_FP64 = 0
+FIELDS_TC_BF16X3 = 1
 _STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_CURAND", 4: "ERR_ALLOC", 5: "ERR_STATE",
            6: "ERR_NUMERIC", 7: "ERR_UNSUPPORTED", 8: "ERR_TIMEOUT"}
 
@@ -106,6 +108,7 @@ def load_library() -> ctypes.CDLL:
         "pspin_fmc_mask": (ctypes.c_int, [ctypes.c_int, vp, ctypes.c_double, vp, vp]),
         "pspin_quartet_roundtrip": (ctypes.c_int, [ctypes.c_int, vp]),
         "pspin_fmc_survivors_static": (ctypes.c_int, [ctypes.c_int, vp, ctypes.c_double, vp, vp]),
+        "pspin_local_fields": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp, vp]),
         "pspin_stream": (vp, [vp]),
         "pspin_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
         "pspin_get_profile": (ctypes.c_int, [vp, vp, vp, vp]),
@@ -300,6 +303,16 @@ class Engine:
         prop = np.empty(NT - 1, np.int64)
         _check(self._lib.pspin_pt_get(self._h, sample, _ptr(perm), _ptr(acc), _ptr(prop)))
         return perm, acc, prop
+
+    # -- all-site local fields ------------------------------------------------------
+    def local_fields(self, sample: int = 0, method: int = 0):
+        """(h [nrep, N] complex, energy [nrep]); method FIELDS_FP64 or FIELDS_TC_BF16X3."""
+        N, R = self.Ns[sample], self.Rs[sample]
+        h = np.empty(2 * N * R, np.float64)
+        e = np.empty(R, np.float64)
+        _check(self._lib.pspin_local_fields(self._h, sample, method, _ptr(h), _ptr(e)))
+        v = h.reshape(R, N, 2)
+        return v[..., 0] + 1j * v[..., 1], e
 
     # -- measurement -------------------------------------------------------------
     def stream_ptr(self) -> int:

@@ -24,7 +24,8 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "noalloc.cu", "layout.cpp"]
+LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "noalloc.cu", "tcfield.cu", "layout.cpp"]
+CUTLASS = "/opt/prime-rl/.venv/lib/python3.12/site-packages/flashinfer/data/cutlass"
 DRIVERS = {
     "pspin_pt": ["drivers/pt_main.cpp"],
     "pspin_pt_sparse": ["drivers/pt_sparse_main.cpp"],
@@ -53,6 +54,7 @@ def build_lib(force: bool = False) -> str:
         return out
     srcs = [os.path.join(CSRC, f) for f in LIB_SOURCES]
     cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-ccbin", HOST_CXX,
+           f"-I{CUTLASS}/include", f"-I{CUTLASS}/tools/util/include", "--expt-relaxed-constexpr",
            "-Xcompiler", "-fPIC,-fopenmp,-O3", "-Xptxas", "-v" if os.environ.get("PSPIN_PTXAS_V") else "-O3",
            "-shared", "-o", out, *srcs, "-lcurand", "-lgomp",
            "-Xlinker", f"-rpath,{CUDA}/lib64"]

@@ -23,7 +23,18 @@
 #include "layout.h"
 #include "rng.cuh"
 
+#include <cuda_bf16.h>
+
 namespace pspin {
+cudaError_t tc_gemm(int M, int NC, int K3, const __nv_bfloat16* A, const __nv_bfloat16* B, float* F, void* workspace,
+                    size_t ws_bytes, cudaStream_t st, size_t* ws_needed);
+cudaError_t launch_split_ws(const float* ws, __nv_bfloat16* out, int M, int Kp, cudaStream_t st);
+cudaError_t launch_pair_split(const float2* spins, int N, int R, int npairs, int Kp, __nv_bfloat16* X,
+                              cudaStream_t st);
+cudaError_t launch_site_fields(const float2* spins, int N, int R, const float* F, int NC, const double* g2,
+                               int h2_active, float2* h, double* e2, double* e4, cudaStream_t st);
+cudaError_t launch_fp64_fields(const float2* spins, int N, int R, const Q64* Q, int64_t nq, const double* g2,
+                               int h2_active, double2* h, cudaStream_t st);
 cudaError_t dev_fmc_mask(uint8_t* mask, const double* omega, int N, double gamma, cudaStream_t st);
 cudaError_t dev_survivor_counts(unsigned long long* counts, const double* omega, int N, double gamma, cudaStream_t st);
 cudaError_t dev_popcount(const uint8_t* mask, int64_t n, unsigned long long* out, cudaStream_t st);
@@ -139,6 +150,17 @@ struct pspin_state {
     unsigned long long* d_drand = nullptr;
     long long *d_ex_acc = nullptr, *d_ex_prop = nullptr;
 
+    // tensor-core all-site fields (one sample at a time)
+    int tc_sample = -1, tc_M = 0, tc_Kp = 0, tc_NC = 0;
+    __nv_bfloat16* d_tc_w = nullptr;     // [M][3Kp]
+    __nv_bfloat16* d_tc_x = nullptr;     // [NC][3Kp]
+    float* d_tc_f = nullptr;             // [M][NC]
+    void* d_tc_ws = nullptr;
+    size_t tc_ws_bytes = 0;
+    float2* d_tc_h = nullptr;
+    double2* d_f64_h = nullptr;
+    double* d_tc_e = nullptr;            // [2][R]
+
     // trace
     pspin_move_record* d_trace = nullptr;
     long long trace_sweep0 = 0;
@@ -158,7 +180,8 @@ static void free_state(pspin_state* s) {
     void* ptrs[] = {s->d_samples, s->d_units, s->d_spins, s->d_E, s->d_beta, s->d_target, s->d_drift,
                     s->d_e2, s->d_e4, s->d_acc, s->d_prop, s->d_key, s->d_entries, s->d_chunk_start, s->d_site_chunks,
                     s->d_q64, s->d_g2, s->d_g4re, s->d_mask, s->d_sweep_counter, s->d_status,
-                    s->d_beta_sched, s->d_perm, s->d_drand, s->d_ex_acc, s->d_ex_prop, s->d_trace};
+                    s->d_beta_sched, s->d_perm, s->d_drand, s->d_ex_acc, s->d_ex_prop, s->d_trace,
+                    s->d_tc_w, s->d_tc_x, s->d_tc_f, s->d_tc_ws, s->d_tc_h, s->d_f64_h, s->d_tc_e};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& e : s->ev_pool) {
@@ -1215,6 +1238,114 @@ extern "C" int pspin_pt_get(pspin_state* s, int sample, int32_t* perm, int64_t* 
 extern "C" int pspin_pt_sweeps_done(pspin_state* s, int64_t* sweeps) {
     if (!s || !sweeps) return fail(PSPIN_ERR_ARG, "null argument");
     *sweeps = s->sweeps_done;
+    return PSPIN_OK;
+}
+
+// ------------------------------------------------------------------ all-site fields
+static int tc_prepare(pspin_state* s, int sample) {
+    if (s->tc_sample == sample) return PSPIN_OK;
+    const SampleHost& h = s->hs[sample];
+    const SampleDev& d = s->sd[sample];
+    const int N = h.N, R = h.R;
+    const int npairs = N * (N - 1) / 2;
+    const int M = (npairs + 127) / 128 * 128, Kp = (npairs + 63) / 64 * 64, NC = (2 * R + 7) / 8 * 8;
+    for (void* p : {(void*)s->d_tc_w, (void*)s->d_tc_x, (void*)s->d_tc_f, s->d_tc_ws, (void*)s->d_tc_h,
+                    (void*)s->d_f64_h, (void*)s->d_tc_e})
+        if (p) cudaFree(p);
+    s->d_tc_w = nullptr; s->d_tc_x = nullptr; s->d_tc_f = nullptr; s->d_tc_ws = nullptr;
+    s->d_tc_h = nullptr; s->d_f64_h = nullptr; s->d_tc_e = nullptr;
+    s->tc_sample = -1;
+    // symmetric pair-space couplings Ws[P][Q] = W[P][Q] + W[Q][P] from the FP64 table
+    std::vector<Q64> q((size_t)d.nq);
+    if (d.nq) CK(cudaMemcpyAsync(q.data(), s->d_q64 + d.q_off, d.nq * sizeof(Q64), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    std::vector<float> ws((size_t)M * Kp, 0.0f);
+    static const int U[3][2] = {{0, 1}, {0, 3}, {0, 2}}, C[3][2] = {{2, 3}, {1, 2}, {1, 3}};
+    auto pidx = [](int a, int b) { return a < b ? b * (b - 1) / 2 + a : a * (a - 1) / 2 + b; };
+    for (const Q64& e : q) {
+        const int ch = e.lch >> 14;
+        const int v[4] = {e.i, e.j, e.k, e.lch & 0x3FFF};
+        const int P = pidx(v[U[ch][0]], v[U[ch][1]]), Q = pidx(v[C[ch][0]], v[C[ch][1]]);
+        ws[(size_t)P * Kp + Q] += (float)e.g;
+        ws[(size_t)Q * Kp + P] += (float)e.g;
+    }
+    float* d_ws32 = nullptr;
+    TRY(dalloc(&d_ws32, ws.size()));
+    int rc = dalloc(&s->d_tc_w, (size_t)M * 3 * Kp);
+    if (rc == PSPIN_OK) rc = dalloc(&s->d_tc_x, (size_t)NC * 3 * Kp);
+    if (rc == PSPIN_OK) rc = dalloc(&s->d_tc_f, (size_t)M * NC);
+    if (rc == PSPIN_OK) rc = dalloc(&s->d_tc_h, (size_t)R * N);
+    if (rc == PSPIN_OK) rc = dalloc(&s->d_f64_h, (size_t)R * N);
+    if (rc == PSPIN_OK) rc = dalloc(&s->d_tc_e, (size_t)2 * R);
+    if (rc == PSPIN_OK) {
+        cudaError_t e = cudaMemcpyAsync(d_ws32, ws.data(), ws.size() * sizeof(float), cudaMemcpyHostToDevice, s->st);
+        if (e == cudaSuccess) e = launch_split_ws(d_ws32, s->d_tc_w, M, Kp, s->st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->d_tc_x, 0, (size_t)NC * 3 * Kp * sizeof(__nv_bfloat16), s->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+        if (e != cudaSuccess) rc = fail(PSPIN_ERR_CUDA, "pair-space couplings: %s", cudaGetErrorString(e));
+    }
+    cudaFree(d_ws32);
+    if (rc != PSPIN_OK) return rc;
+    size_t need = 0;
+    CK(tc_gemm(M, NC, 3 * Kp, nullptr, nullptr, nullptr, nullptr, 0, s->st, &need));
+    if (need) TRY(dalloc((char**)&s->d_tc_ws, need));
+    s->tc_ws_bytes = need;
+    s->tc_sample = sample;
+    s->tc_M = M;
+    s->tc_Kp = Kp;
+    s->tc_NC = NC;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_local_fields(pspin_state* s, int sample, int method, double* h, double* energy) {
+    if (!s || !h || sample < 0 || sample >= s->S) return fail(PSPIN_ERR_ARG, "bad arguments");
+    if (s->variant != PSPIN_DENSE) return fail(PSPIN_ERR_UNSUPPORTED, "all-site fields: dense variant only");
+    const SampleHost& hs = s->hs[sample];
+    const SampleDev& d = s->sd[sample];
+    const int N = hs.N, R = hs.R;
+    const float2* spins = s->d_spins + d.spin_off;
+    const double* g2 = s->d_g2 + d.g2_off;
+    std::vector<double> e(2 * (size_t)R, 0.0);
+    if (method == PSPIN_FIELDS_FP64) {
+        if (!s->d_f64_h || s->tc_sample != sample) {
+            // fields only: the scratch of the tensor-core path is not needed
+            if (s->d_f64_h) cudaFree(s->d_f64_h);
+            s->d_f64_h = nullptr;
+            TRY(dalloc(&s->d_f64_h, (size_t)R * N));
+            s->tc_sample = -2;   // the tensor-core buffers (if any) belong to no sample now
+        }
+        CK(launch_fp64_fields(spins, N, R, s->d_q64 + d.q_off, d.nq, g2, hs.h2_active, s->d_f64_h, s->st));
+        s->kernel_launches++;
+        std::vector<double2> hv((size_t)R * N);
+        CK(cudaMemcpyAsync(hv.data(), s->d_f64_h, hv.size() * sizeof(double2), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        for (size_t t = 0; t < hv.size(); t++) { h[2 * t] = hv[t].x; h[2 * t + 1] = hv[t].y; }
+        if (energy) {
+            std::vector<double> e2(R), e4(R);
+            TRY(run_energy(s, s->d_e2, s->d_e4, false, false));
+            CK(cudaMemcpyAsync(e2.data(), s->d_e2 + d.rep_off, R * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+            CK(cudaMemcpyAsync(e4.data(), s->d_e4 + d.rep_off, R * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+            for (int r = 0; r < R; r++) energy[r] = e2[r] + e4[r];
+        }
+        return PSPIN_OK;
+    }
+    if (method != PSPIN_FIELDS_TC_BF16X3) return fail(PSPIN_ERR_ARG, "unknown field method %d", method);
+    TRY(tc_prepare(s, sample));
+    const int npairs = N * (N - 1) / 2;
+    CK(launch_pair_split(spins, N, R, npairs, s->tc_Kp, s->d_tc_x, s->st));
+    CK(tc_gemm(s->tc_M, s->tc_NC, 3 * s->tc_Kp, s->d_tc_w, s->d_tc_x, s->d_tc_f, s->d_tc_ws, s->tc_ws_bytes, s->st,
+               nullptr));
+    CK(launch_site_fields(spins, N, R, s->d_tc_f, s->tc_NC, g2, hs.h2_active, s->d_tc_h, s->d_tc_e,
+                          s->d_tc_e + R, s->st));
+    s->kernel_launches += 3;
+    std::vector<float2> hv((size_t)R * N);
+    CK(cudaMemcpyAsync(hv.data(), s->d_tc_h, hv.size() * sizeof(float2), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(e.data(), s->d_tc_e, 2 * R * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (size_t t = 0; t < hv.size(); t++) { h[2 * t] = hv[t].x; h[2 * t + 1] = hv[t].y; }
+    if (energy)
+        for (int r = 0; r < R; r++) energy[r] = e[r] + e[R + r];
     return PSPIN_OK;
 }
 

@@ -154,6 +154,16 @@ int  pspin_pt_run(pspin_state* s, int nsweeps);
 int  pspin_pt_get(pspin_state* s, int sample, int32_t* perm, int64_t* ex_acc, int64_t* ex_prop);
 int  pspin_pt_sweeps_done(pspin_state* s, int64_t* sweeps);
 
+/* ---- all-site local fields (no reference counterpart) ----------------- */
+enum { PSPIN_FIELDS_FP64 = 0,      /* FP64 sum over the quartet table */
+       PSPIN_FIELDS_TC_BF16X3 = 1  /* tcgen05 contraction, split-BF16 operands, FP32 accumulate */ };
+/* Local field h_m of every site of every replica of one dense sample
+ * (dE of a one-site change = -Re[da_m h_m]) and the energy computed from
+ * the fields.  h [nrep][N][re,im], energy [nrep] (may be NULL).  The
+ * tensor-core method builds the symmetric pair-space coupling matrix on its
+ * first call for the sample (C(N,2)^2 BF16 x 3 on the device). */
+int  pspin_local_fields(pspin_state* s, int sample, int method, double* h, double* energy);
+
 /* ---- per-move trace (tests) ------------------------------------------ */
 int  pspin_trace_get(pspin_state* s, pspin_move_record* out, int max_records, int* n_records);
 
