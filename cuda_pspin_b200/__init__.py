@@ -27,6 +27,11 @@ PSPIN_DENSE = 0
 PSPIN_SPARSE = 1
 FIELDS_FP64 = 0
 FIELDS_TC_BF16X3 = 1
+PROPOSAL_PLAIN = 0
+PROPOSAL_PLAIN_FIELDS = 1
+PROPOSAL_LEARNED = 2
+MLP_PARAMS = 6426
+RECORD_FLOATS = 11
 _STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_CURAND", 4: "ERR_ALLOC", 5: "ERR_STATE",
            6: "ERR_NUMERIC", 7: "ERR_UNSUPPORTED", 8: "ERR_TIMEOUT"}
 
@@ -64,7 +69,8 @@ class Info(ctypes.Structure):
 
 MOVE_RECORD = np.dtype([("i0", np.int32), ("j0", np.int32), ("ai_old", np.float32, 2),
                         ("aj_old", np.float32, 2), ("ai_new", np.float32, 2), ("aj_new", np.float32, 2),
-                        ("dE", np.float32), ("accepted", np.int32)])
+                        ("dE", np.float32), ("accepted", np.int32), ("log_q_ratio", np.float32),
+                        ("log_u", np.float32)])
 
 _lib = None
 
@@ -109,6 +115,12 @@ def load_library() -> ctypes.CDLL:
         "pspin_quartet_roundtrip": (ctypes.c_int, [ctypes.c_int, vp]),
         "pspin_fmc_survivors_static": (ctypes.c_int, [ctypes.c_int, vp, ctypes.c_double, vp, vp]),
         "pspin_local_fields": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp, vp]),
+        "pspin_set_proposal": (ctypes.c_int, [vp, ctypes.c_int]),
+        "pspin_learn_init": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_float]),
+        "pspin_learn_params": (ctypes.c_int, [vp, vp, vp]),
+        "pspin_learn_train": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, vp]),
+        "pspin_learn_records": (ctypes.c_int, [vp, vp, vp, ctypes.c_int]),
+        "pspin_learn_loss_grad": (ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp]),
         "pspin_stream": (vp, [vp]),
         "pspin_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
         "pspin_get_profile": (ctypes.c_int, [vp, vp, vp, vp]),
@@ -313,6 +325,39 @@ class Engine:
         _check(self._lib.pspin_local_fields(self._h, sample, method, _ptr(h), _ptr(e)))
         v = h.reshape(R, N, 2)
         return v[..., 0] + 1j * v[..., 1], e
+
+    # -- learned proposal -------------------------------------------------------------
+    def set_proposal(self, proposal: int) -> None:
+        _check(self._lib.pspin_set_proposal(self._h, int(proposal)))
+
+    def learn_init(self, seed: int = 1, capacity: int = 1 << 20, record_prob: float = 1.0) -> None:
+        _check(self._lib.pspin_learn_init(self._h, int(seed), int(capacity), float(record_prob)))
+
+    def learn_params(self, set_to=None) -> np.ndarray:
+        out = np.empty(MLP_PARAMS, np.float32)
+        src = None if set_to is None else _ptr(np.ascontiguousarray(set_to, np.float32))
+        _check(self._lib.pspin_learn_params(self._h, _ptr(out), src))
+        if set_to is not None:
+            out = np.ascontiguousarray(set_to, np.float32).copy()
+        return out
+
+    def learn_train(self, steps: int, batch: int = 4096, lr: float = 1e-3) -> float:
+        loss = ctypes.c_double(0)
+        _check(self._lib.pspin_learn_train(self._h, int(steps), int(batch), float(lr), ctypes.byref(loss)))
+        return loss.value
+
+    def learn_records(self, max_records: int = 0):
+        n = ctypes.c_int64(0)
+        out = np.empty((max(max_records, 1), RECORD_FLOATS), np.float32)
+        _check(self._lib.pspin_learn_records(self._h, ctypes.byref(n), _ptr(out), int(max_records)))
+        return n.value, out[:min(max_records, n.value)]
+
+    def learn_loss_grad(self, records: np.ndarray):
+        r = np.ascontiguousarray(records, np.float32)
+        loss = ctypes.c_double(0)
+        g = np.empty(MLP_PARAMS, np.float32)
+        _check(self._lib.pspin_learn_loss_grad(self._h, _ptr(r), len(r), ctypes.byref(loss), _ptr(g)))
+        return loss.value, g
 
     # -- measurement -------------------------------------------------------------
     def stream_ptr(self) -> int:

@@ -24,7 +24,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "noalloc.cu", "tcfield.cu", "layout.cpp"]
+LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "noalloc.cu", "tcfield.cu", "learned.cu", "layout.cpp"]
 CUTLASS = "/opt/prime-rl/.venv/lib/python3.12/site-packages/flashinfer/data/cutlass"
 DRIVERS = {
     "pspin_pt": ["drivers/pt_main.cpp"],
@@ -46,19 +46,29 @@ def _newer(target: str, deps: list[str]) -> bool:
 
 
 def build_lib(force: bool = False) -> str:
+    """Compiles every source to an object under _build/ (skipped when newer
+    than the source and the shared headers) and links libpspin.so."""
     os.makedirs(LIB_DIR, exist_ok=True)
+    obj_dir = os.path.join(ROOT, "_build", "obj")
+    os.makedirs(obj_dir, exist_ok=True)
     out = os.path.join(LIB_DIR, "libpspin.so")
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp", ".h", ".cuh"))]
-    deps.append(os.path.join(ROOT, "include", "pspin.h"))
-    if not force and not _newer(out, deps):
-        return out
-    srcs = [os.path.join(CSRC, f) for f in LIB_SOURCES]
-    cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-ccbin", HOST_CXX,
-           f"-I{CUTLASS}/include", f"-I{CUTLASS}/tools/util/include", "--expt-relaxed-constexpr",
-           "-Xcompiler", "-fPIC,-fopenmp,-O3", "-Xptxas", "-v" if os.environ.get("PSPIN_PTXAS_V") else "-O3",
-           "-shared", "-o", out, *srcs, "-lcurand", "-lgomp",
-           "-Xlinker", f"-rpath,{CUDA}/lib64"]
-    _run(cmd)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(ROOT, "include", "pspin.h"))
+    flags = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-ccbin", HOST_CXX,
+             f"-I{CUTLASS}/include", f"-I{CUTLASS}/tools/util/include", "--expt-relaxed-constexpr",
+             "-diag-suppress", "20012", "-Xcompiler", "-fPIC,-fopenmp,-O3"]
+    if os.environ.get("PSPIN_PTXAS_V"):
+        flags += ["-Xptxas", "-v"]
+    objs = []
+    for f in LIB_SOURCES:
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(obj_dir, f + ".o")
+        objs.append(obj)
+        if force or _newer(obj, [src, *headers]):
+            _run([*flags, "-c", src, "-o", obj])
+    if force or _newer(out, objs):
+        _run([NVCC, *ARCH, "-ccbin", HOST_CXX, "-shared", "-o", out, *objs, "-lcurand", "-lgomp",
+              "-Xlinker", f"-rpath,{CUDA}/lib64"])
     return out
 
 

@@ -35,6 +35,24 @@ cudaError_t launch_site_fields(const float2* spins, int N, int R, const float* F
                                int h2_active, float2* h, double* e2, double* e4, cudaStream_t st);
 cudaError_t launch_fp64_fields(const float2* spins, int N, int R, const Q64* Q, int64_t nq, const double* g2,
                                int h2_active, double2* h, cudaStream_t st);
+struct LearnParams {
+    int mode;
+    const __nv_bfloat16* w;
+    float* records;
+    unsigned long long* rec_count;
+    int rec_cap;
+    float rec_prob;
+};
+cudaError_t launch_learned_sweep(const SweepParams& p, const LearnParams& l, int n_units, int max_N, cudaStream_t st);
+cudaError_t launch_mlp_fwd_bwd(const float* w, const float* records, const int* index, int n, float* save,
+                               float* loss, cudaStream_t st);
+cudaError_t launch_mlp_grad(const float* save, int n, float* grad, cudaStream_t st);
+cudaError_t launch_adam(float* w, float* m, float* v, const float* g, __nv_bfloat16* wbf, float lr, int t,
+                        cudaStream_t st);
+cudaError_t launch_to_bf16(const float* w, __nv_bfloat16* wbf, cudaStream_t st);
+cudaError_t launch_sample_index(int* idx, int n, unsigned long long filled, uint64_t key, uint32_t step,
+                                cudaStream_t st);
+constexpr int kMlpParamsHost = 6426, kRecordFloatsHost = 11, kSaveFloatsHost = 8 + 4 * 64 + 26;
 cudaError_t dev_fmc_mask(uint8_t* mask, const double* omega, int N, double gamma, cudaStream_t st);
 cudaError_t dev_survivor_counts(unsigned long long* counts, const double* omega, int N, double gamma, cudaStream_t st);
 cudaError_t dev_popcount(const uint8_t* mask, int64_t n, unsigned long long* out, cudaStream_t st);
@@ -161,6 +179,20 @@ struct pspin_state {
     double2* d_f64_h = nullptr;
     double* d_tc_e = nullptr;            // [2][R]
 
+    // learned proposal
+    int proposal = PSPIN_PROPOSAL_PLAIN;
+    float *d_w32 = nullptr, *d_adam_m = nullptr, *d_adam_v = nullptr, *d_grad = nullptr;
+    __nv_bfloat16* d_wbf = nullptr;
+    float* d_records = nullptr;
+    unsigned long long* d_rec_count = nullptr;
+    int rec_cap = 0;
+    float rec_prob = 0.f;
+    float *d_save = nullptr, *d_loss = nullptr;
+    int* d_idx = nullptr;
+    int save_cap = 0;
+    int adam_t = 0;
+    uint64_t learn_seed = 0;
+
     // trace
     pspin_move_record* d_trace = nullptr;
     long long trace_sweep0 = 0;
@@ -181,7 +213,9 @@ static void free_state(pspin_state* s) {
                     s->d_e2, s->d_e4, s->d_acc, s->d_prop, s->d_key, s->d_entries, s->d_chunk_start, s->d_site_chunks,
                     s->d_q64, s->d_g2, s->d_g4re, s->d_mask, s->d_sweep_counter, s->d_status,
                     s->d_beta_sched, s->d_perm, s->d_drand, s->d_ex_acc, s->d_ex_prop, s->d_trace,
-                    s->d_tc_w, s->d_tc_x, s->d_tc_f, s->d_tc_ws, s->d_tc_h, s->d_f64_h, s->d_tc_e};
+                    s->d_tc_w, s->d_tc_x, s->d_tc_f, s->d_tc_ws, s->d_tc_h, s->d_f64_h, s->d_tc_e,
+                    s->d_w32, s->d_adam_m, s->d_adam_v, s->d_grad, s->d_wbf, s->d_records, s->d_rec_count,
+                    s->d_save, s->d_loss, s->d_idx};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& e : s->ev_pool) {
@@ -987,7 +1021,18 @@ static int launch_chunk(pspin_state* s, int nsweeps, bool exchange) {
         s->ev_used++;
         CK(cudaEventRecord(e0, s->st));
     }
-    CK(launch_sweep(p, (int)s->units.size(), s->variant, s->max_N, s->st));
+    if (s->proposal == PSPIN_PROPOSAL_PLAIN) {
+        CK(launch_sweep(p, (int)s->units.size(), s->variant, s->max_N, s->st));
+    } else {
+        LearnParams lp{};
+        lp.mode = s->proposal;
+        lp.w = s->d_wbf;
+        lp.records = s->d_records;
+        lp.rec_count = s->d_rec_count;
+        lp.rec_cap = s->rec_cap;
+        lp.rec_prob = s->rec_prob;
+        CK(launch_learned_sweep(p, lp, (int)s->units.size(), s->max_N, s->st));
+    }
     if (s->profiling) CK(cudaEventRecord(e1, s->st));
     s->sweep_launches++;
     s->kernel_launches++;
@@ -1346,6 +1391,165 @@ extern "C" int pspin_local_fields(pspin_state* s, int sample, int method, double
     for (size_t t = 0; t < hv.size(); t++) { h[2 * t] = hv[t].x; h[2 * t + 1] = hv[t].y; }
     if (energy)
         for (int r = 0; r < R; r++) energy[r] = e[r] + e[R + r];
+    return PSPIN_OK;
+}
+
+// ------------------------------------------------------------------ learned proposal
+extern "C" int pspin_set_proposal(pspin_state* s, int proposal) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (proposal < PSPIN_PROPOSAL_PLAIN || proposal > PSPIN_PROPOSAL_LEARNED)
+        return fail(PSPIN_ERR_ARG, "unknown proposal %d", proposal);
+    if (proposal != PSPIN_PROPOSAL_PLAIN && s->variant != PSPIN_DENSE)
+        return fail(PSPIN_ERR_UNSUPPORTED, "the learned proposal is built for the dense (spherical) variant");
+    if (proposal == PSPIN_PROPOSAL_LEARNED && !s->d_wbf)
+        return fail(PSPIN_ERR_STATE, "pspin_learn_init has not been called");
+    s->proposal = proposal;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_learn_init(pspin_state* s, uint64_t seed, int capacity, float record_prob) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (capacity < 1) return fail(PSPIN_ERR_ARG, "record capacity must be >= 1");
+    for (void* p : {(void*)s->d_w32, (void*)s->d_adam_m, (void*)s->d_adam_v, (void*)s->d_grad, (void*)s->d_wbf,
+                    (void*)s->d_records, (void*)s->d_rec_count})
+        if (p) cudaFree(p);
+    s->d_w32 = s->d_adam_m = s->d_adam_v = s->d_grad = nullptr;
+    s->d_wbf = nullptr;
+    s->d_records = nullptr;
+    s->d_rec_count = nullptr;
+    const int P = kMlpParamsHost;
+    int rc;
+    if ((rc = dalloc(&s->d_w32, P)) || (rc = dalloc(&s->d_adam_m, P)) || (rc = dalloc(&s->d_adam_v, P)) ||
+        (rc = dalloc(&s->d_grad, P)) || (rc = dalloc(&s->d_wbf, P)) ||
+        (rc = dalloc(&s->d_records, (size_t)capacity * kRecordFloatsHost)) || (rc = dalloc(&s->d_rec_count, 1)))
+        return rc;
+    // Xavier-uniform weights; biases 0 except the mixtures: means spread over
+    // the circle, concentrations low (kappa ~ 1)
+    std::vector<float> w(P, 0.0f);
+    uint64_t st = seed;
+    auto uni = [&]() { return (double)(splitmix64(st) >> 11) / 9007199254740992.0; };
+    auto fill = [&](int off, int fan_out, int fan_in) {
+        const double a = std::sqrt(6.0 / (fan_in + fan_out));
+        for (int t = 0; t < fan_out * fan_in; t++) w[off + t] = (float)((2.0 * uni() - 1.0) * a);
+    };
+    fill(0, 64, 8);
+    fill(8 * 64 + 64, 64, 64);
+    const int offW3 = 8 * 64 + 64 + 64 * 64 + 64, offB3 = offW3 + 26 * 64;
+    fill(offW3, 26, 64);
+    for (int t = 0; t < 26 * 64; t++) w[offW3 + t] *= 0.1f;
+    for (int sdx = 0; sdx < 2; sdx++)
+        for (int k = 0; k < 4; k++) {
+            w[offB3 + 2 + 12 * sdx + 4 + k] = (float)(k * 1.5707963267948966 - 2.356194490192345);
+            w[offB3 + 2 + 12 * sdx + 8 + k] = -3.9f;
+        }
+    CK(cudaMemcpyAsync(s->d_w32, w.data(), P * sizeof(float), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemsetAsync(s->d_adam_m, 0, P * sizeof(float), s->st));
+    CK(cudaMemsetAsync(s->d_adam_v, 0, P * sizeof(float), s->st));
+    CK(cudaMemsetAsync(s->d_rec_count, 0, sizeof(unsigned long long), s->st));
+    CK(launch_to_bf16(s->d_w32, s->d_wbf, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    s->rec_cap = capacity;
+    s->rec_prob = record_prob;
+    s->adam_t = 0;
+    s->learn_seed = seed;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_learn_params(pspin_state* s, float* get, const float* set) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (!s->d_w32) return fail(PSPIN_ERR_STATE, "pspin_learn_init has not been called");
+    if (get) CK(cudaMemcpyAsync(get, s->d_w32, kMlpParamsHost * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+    if (set) {
+        CK(cudaMemcpyAsync(s->d_w32, set, kMlpParamsHost * sizeof(float), cudaMemcpyHostToDevice, s->st));
+        CK(launch_to_bf16(s->d_w32, s->d_wbf, s->st));
+    }
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+static int ensure_save(pspin_state* s, int n) {
+    if (n <= s->save_cap) return PSPIN_OK;
+    cudaFree(s->d_save);
+    cudaFree(s->d_loss);
+    cudaFree(s->d_idx);
+    s->d_save = nullptr; s->d_loss = nullptr; s->d_idx = nullptr;
+    s->save_cap = 0;
+    int rc;
+    if ((rc = dalloc(&s->d_save, (size_t)n * kSaveFloatsHost)) || (rc = dalloc(&s->d_loss, n)) ||
+        (rc = dalloc(&s->d_idx, n)))
+        return rc;
+    s->save_cap = n;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_learn_train(pspin_state* s, int steps, int batch, float lr, double* mean_loss) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (!s->d_w32) return fail(PSPIN_ERR_STATE, "pspin_learn_init has not been called");
+    if (steps < 0 || batch < 1) return fail(PSPIN_ERR_ARG, "bad steps/batch");
+    unsigned long long cnt = 0;
+    CK(cudaMemcpyAsync(&cnt, s->d_rec_count, sizeof(cnt), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    const unsigned long long filled = cnt < (unsigned long long)s->rec_cap ? cnt : (unsigned long long)s->rec_cap;
+    if (filled == 0) return fail(PSPIN_ERR_STATE, "no training records yet");
+    TRY(ensure_save(s, batch));
+    for (int it = 0; it < steps; it++) {
+        CK(launch_sample_index(s->d_idx, batch, filled, s->learn_seed ^ 0x5eedULL, (uint32_t)s->adam_t, s->st));
+        CK(launch_mlp_fwd_bwd(s->d_w32, s->d_records, s->d_idx, batch, s->d_save, s->d_loss, s->st));
+        CK(launch_mlp_grad(s->d_save, batch, s->d_grad, s->st));
+        s->adam_t++;
+        CK(launch_adam(s->d_w32, s->d_adam_m, s->d_adam_v, s->d_grad, s->d_wbf, lr, s->adam_t, s->st));
+        s->kernel_launches += 4;
+    }
+    if (mean_loss) {
+        std::vector<float> l(batch);
+        CK(cudaMemcpyAsync(l.data(), s->d_loss, batch * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        double m = 0.0;
+        for (float v : l) m += v;
+        *mean_loss = m / batch;
+    }
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_learn_records(pspin_state* s, int64_t* n_recorded, float* out, int max) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (!s->d_rec_count) return fail(PSPIN_ERR_STATE, "pspin_learn_init has not been called");
+    unsigned long long cnt = 0;
+    CK(cudaMemcpyAsync(&cnt, s->d_rec_count, sizeof(cnt), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (n_recorded) *n_recorded = (int64_t)cnt;
+    if (out && max > 0) {
+        const unsigned long long n = std::min<unsigned long long>(
+            std::min<unsigned long long>(cnt, (unsigned long long)s->rec_cap), (unsigned long long)max);
+        CK(cudaMemcpyAsync(out, s->d_records, n * kRecordFloatsHost * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_learn_loss_grad(pspin_state* s, const float* records, int n, double* loss, float* grad) {
+    if (!s || !records || n < 1) return fail(PSPIN_ERR_ARG, "bad arguments");
+    if (!s->d_w32) return fail(PSPIN_ERR_STATE, "pspin_learn_init has not been called");
+    TRY(ensure_save(s, n));
+    float* d_rec = nullptr;
+    TRY(dalloc(&d_rec, (size_t)n * kRecordFloatsHost));
+    cudaError_t e = cudaMemcpyAsync(d_rec, records, (size_t)n * kRecordFloatsHost * sizeof(float),
+                                    cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = launch_mlp_fwd_bwd(s->d_w32, d_rec, nullptr, n, s->d_save, s->d_loss, s->st);
+    if (e == cudaSuccess) e = launch_mlp_grad(s->d_save, n, s->d_grad, s->st);
+    std::vector<float> l(n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(l.data(), s->d_loss, n * sizeof(float), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess && grad)
+        e = cudaMemcpyAsync(grad, s->d_grad, kMlpParamsHost * sizeof(float), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    cudaFree(d_rec);
+    if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "loss/grad: %s", cudaGetErrorString(e));
+    if (loss) {
+        double m = 0.0;
+        for (float v : l) m += v;
+        *loss = m / n;
+    }
     return PSPIN_OK;
 }
 

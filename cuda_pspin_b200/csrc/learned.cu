@@ -1,0 +1,420 @@
+// learned.cu -- the sweep with local fields at both ends of every move, used
+// (mode 1) to record accepted plain moves for training and (mode 2) to run
+// the learned proposal with the exact Metropolis-Hastings correction; and
+// the network's training kernels (forward, backward, Adam).
+//
+// Two field passes per move.  Pass 1 reads site i's and site j's lists at
+// the current state x: h_i(x), h_j(x) (the proposal's features).  The
+// proposal is then written into both slots and pass 2 gives h_i(x'), h_j(x')
+// (the reverse density's features).  E is affine in each site, so
+//     dE = -Re[da_i h_i(x')] - Re[da_j h_j(x)]
+// exactly (h_i(x') is h_i with a_j' in place, h_j(x) is h_j with a_i).
+#include <cuda_bf16.h>
+
+#include "../../include/pspin.h"
+#include "mlp.cuh"
+#include "sweep_common.cuh"
+
+namespace pspin {
+
+struct LearnParams {
+    int mode;                       // 1: plain proposal, fields + recording; 2: learned proposal
+    const __nv_bfloat16* w;         // network weights [kMlpParams]
+    float* records;                 // ring of accepted plain moves [cap][kRecordFloats]
+    unsigned long long* rec_count;  // moves written so far (ring position = count % cap)
+    int rec_cap;
+    float rec_prob;
+};
+
+// Inference for the 32 replicas of warp 0: activations in shared memory
+// [64][32] (lane-contiguous), weights in shared memory (BF16, broadcast reads).
+__device__ __forceinline__ void mlp_warp(const __nv_bfloat16* __restrict__ w, const float* f, float* act1,
+                                         float* act2, int lane, float* out) {
+    for (int o = 0; o < kMlpHidden; o++) {
+        float z = __bfloat162float(w[kOffB1 + o]);
+#pragma unroll
+        for (int i = 0; i < kMlpIn; i++) z = fmaf(__bfloat162float(w[kOffW1 + o * kMlpIn + i]), f[i], z);
+        act1[o * 32 + lane] = tanhf(z);
+    }
+    for (int o = 0; o < kMlpHidden; o++) {
+        float z = __bfloat162float(w[kOffB2 + o]);
+#pragma unroll 8
+        for (int i = 0; i < kMlpHidden; i++)
+            z = fmaf(__bfloat162float(w[kOffW2 + o * kMlpHidden + i]), act1[i * 32 + lane], z);
+        act2[o * 32 + lane] = tanhf(z);
+    }
+    for (int o = 0; o < kMlpOut; o++) {
+        float z = __bfloat162float(w[kOffB3 + o]);
+#pragma unroll 8
+        for (int i = 0; i < kMlpHidden; i++)
+            z = fmaf(__bfloat162float(w[kOffW3 + o * kMlpHidden + i]), act2[i * 32 + lane], z);
+        out[o] = z;
+    }
+}
+
+__device__ __forceinline__ float argf(float2 a) { return atan2f(a.y, a.x); }
+
+inline size_t learned_smem_bytes(int N, int warps) {
+    return sweep_smem_bytes(N, warps) + (size_t)kMlpParams * sizeof(__nv_bfloat16) + 16 +
+           (size_t)2 * kMlpHidden * 32 * sizeof(float);
+}
+
+__global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams P, const LearnParams L) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Unit U = P.units[blockIdx.x];
+    const SampleDev S = P.samples[U.sample];
+    const int N = S.N, R = S.R;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = P.warps;
+    float2* sp = reinterpret_cast<float2*>(smem_raw);
+    float4* red = reinterpret_cast<float4*>(sp + (size_t)(N + 1) * kRepBlock);
+    int2* ring_all = reinterpret_cast<int2*>(red + (size_t)W * kRepBlock);
+    int2* ring = ring_all + (size_t)warp * kStages * kStage;
+    uint64_t* bars_all = reinterpret_cast<uint64_t*>(ring_all + (size_t)W * kStages * kStage);
+    uint64_t* bars = bars_all + warp * kStages;
+    float* act1 = reinterpret_cast<float*>(bars_all + W * kStages);
+    float* act2 = act1 + kMlpHidden * 32;
+    __nv_bfloat16* wsm = reinterpret_cast<__nv_bfloat16*>(act2 + kMlpHidden * 32);
+
+    const bool active = lane < U.rep_count;
+    const int64_t gr = S.rep_off + U.rep_begin + lane;
+    for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
+        const int site = idx >> 5, l = idx & 31;
+        float2 v = make_float2(1.f, 0.f);
+        if (l < U.rep_count) v = P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l];
+        sp[idx] = v;
+    }
+    if (threadIdx.x < kRepBlock) sp[N * kRepBlock + threadIdx.x] = make_float2(1.f, 0.f);
+    if (L.mode == 2)
+        for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) wsm[i] = L.w[i];
+
+    double E = 0.0, beta_d = 0.0;
+    float beta = 0.f;
+    long long nacc = 0, nprop = 0;
+    uint32_t k0 = 0, k1 = 0;
+    if (warp == 0 && active) {
+        E = P.energy[gr];
+        beta_d = P.beta[gr];
+        beta = (float)beta_d;
+        const uint64_t key = P.key[gr];
+        k0 = (uint32_t)key;
+        k1 = (uint32_t)(key >> 32);
+    }
+    const long long sweep0 = *P.sweep_counter;
+    const int steps = N / 2, total = P.nsweeps * steps;
+    Stream st;
+    st.key0 = S.pair_key0;
+    st.key1 = S.pair_key1;
+    st.N = N;
+    st.site_chunks = P.site_chunks + S.split_off;
+    st.sweep0 = sweep0;
+    st.steps = steps;
+    st.total = total;
+    st.part0 = warp * (kSplit / W);
+    st.part1 = (warp + 1) * (kSplit / W);
+    st.lists = 4;
+    if (lane == 0) {
+        for (int s = 0; s < kStages; s++) mbar_init(bars + s, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        fence_async_shared();
+    }
+    __syncwarp();
+    Cursor pc = st.first();
+    uint32_t issued = 0, consumed = 0;
+    bool ok_wait = true;
+    auto issue = [&]() {
+        if (pc.m >= total) return;
+        const uint32_t slot = issued % kStages;
+        if (lane == 0) {
+            const int64_t b = __ldg(P.chunk_start + pc.c), e = __ldg(P.chunk_start + pc.c + 1);
+            const uint32_t bytes = (uint32_t)((e - b) * sizeof(int2));
+            mbar_expect_tx(bars + slot, bytes);
+            bulk_g2s(ring + slot * kStage, P.entries + b, bytes, bars + slot);
+        }
+        issued++;
+        st.next(pc);
+    };
+    for (int s = 0; s < kStages; s++) issue();
+    __syncthreads();
+
+    // one field pass over this warp's share of site i0's and site j0's lists
+    auto pass = [&](int m, int base, float* h) {
+        for (int which = base; which < base + 2; which++) {
+            int c, c_end;
+            st.range(m, which, c, c_end);
+            for (; c < c_end; c++) {
+                const uint32_t slot = consumed % kStages;
+                if (ok_wait) ok_wait = mbar_wait(bars + slot, (consumed / kStages) & 1u, P.status);
+                const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
+                const int k2 = 2 * (which & 1);
+                if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
+                else accumulate_chunk(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
+                consumed++;
+                __syncwarp();
+                if (lane == 0) fence_async_shared();
+                issue();
+            }
+        }
+    };
+
+    for (int m = 0; m < total; m++) {
+        const long long sw = sweep0 + m / steps;
+        const int k = m % steps;
+        int i0, j0;
+        pair_pick(S.pair_key0, S.pair_key1, (uint64_t)sw, (uint32_t)k, N, i0, j0);
+
+        float h[4] = {0.f, 0.f, 0.f, 0.f};
+        pass(m, 0, h);
+        red[warp * kRepBlock + lane] = make_float4(h[0], h[1], h[2], h[3]);
+        __syncthreads();
+
+        // ---- proposal (warp 0) -------------------------------------------------
+        float2 ai = make_float2(0.f, 0.f), aj = ai, ain = ai, ajn = ai, hi1 = ai, hj1 = ai;
+        float cu = 0.f, lq_fwd = 0.f, lq_ratio = 0.f, tn = 0.5f, psi_i = 0.f, psi_j = 0.f;
+        bool ok = true;
+        MoveStream g;
+        if (warp == 0) {
+            float4 hs = red[lane];
+            for (int w = 1; w < W; w++) {
+                const float4 v = red[w * kRepBlock + lane];
+                hs.x += v.x; hs.y += v.y; hs.z += v.z; hs.w += v.w;
+            }
+            hi1 = make_float2(hs.x, hs.y);
+            hj1 = make_float2(hs.z, hs.w);
+            ai = sp[i0 * kRepBlock + lane];
+            aj = sp[j0 * kRepBlock + lane];
+            const float Ssum = fmaf(ai.x, ai.x, ai.y * ai.y) + fmaf(aj.x, aj.x, aj.y * aj.y);
+            g = MoveStream{k0, k1, (uint32_t)k, (uint32_t)sw, (uint32_t)((uint64_t)sw >> 32), 0u, 4u, U4{0, 0, 0, 0}};
+            if (L.mode == 1) {
+                const U4 w = move_words(k0, k1, (uint64_t)sw, (uint32_t)k);
+                propose<0>(ai, aj, w, ain, ajn);
+                cu = u01f(w.w);
+                tn = fmaf(ain.x, ain.x, ain.y * ain.y) / Ssum;
+                psi_i = argf(ain) + argf(hi1);
+                psi_j = argf(ajn) + argf(hj1);
+            } else {
+                float f[kMlpIn], out[kMlpOut];
+                pair_features(ai, aj, hi1, hj1, beta, f);
+                mlp_warp(wsm, f, act1, act2, lane, out);
+                ProposalParams pp;
+                decode_outputs(out, pp);
+                ok = sample_move(g, pp, tn, psi_i, psi_j);
+                if (ok) {
+                    const float mi = sqrtf(Ssum * tn), mj = sqrtf(Ssum * (1.0f - tn));
+                    float s1, c1, s2, c2;
+                    sincosf(psi_i - argf(hi1), &s1, &c1);
+                    sincosf(psi_j - argf(hj1), &s2, &c2);
+                    ain = make_float2(mi * c1, mi * s1);
+                    ajn = make_float2(mj * c2, mj * s2);
+                    lq_fwd = log_learned_density(pp, tn, psi_i, psi_j) - log_plain_density(tn);
+                } else {
+                    ain = ai;
+                    ajn = aj;
+                }
+                cu = g.uniform();
+            }
+            sp[i0 * kRepBlock + lane] = ain;
+            sp[j0 * kRepBlock + lane] = ajn;
+        }
+        __syncthreads();
+
+        // ---- fields at the proposed state ---------------------------------------
+        h[0] = h[1] = h[2] = h[3] = 0.f;
+        pass(m, 2, h);
+        red[warp * kRepBlock + lane] = make_float4(h[0], h[1], h[2], h[3]);
+        __syncthreads();
+
+        if (warp == 0) {
+            float4 hs = red[lane];
+            for (int w = 1; w < W; w++) {
+                const float4 v = red[w * kRepBlock + lane];
+                hs.x += v.x; hs.y += v.y; hs.z += v.z; hs.w += v.w;
+            }
+            const float2 hi2 = make_float2(hs.x, hs.y), hj2 = make_float2(hs.z, hs.w);
+            const float dix = ain.x - ai.x, diy = ain.y - ai.y, djx = ajn.x - aj.x, djy = ajn.y - aj.y;
+            const float dE = -fmaf(dix, hi2.x, -diy * hi2.y) - fmaf(djx, hj1.x, -djy * hj1.y);
+            bool accept;
+            if (L.mode == 1) {
+                if (beta_d == 0.0) accept = true;
+                else accept = (dE <= 0.f) || (cu < expf(-beta * dE));
+            } else {
+                float f[kMlpIn], out[kMlpOut];
+                pair_features(ain, ajn, hi2, hj2, beta, f);
+                mlp_warp(wsm, f, act1, act2, lane, out);
+                ProposalParams pr;
+                decode_outputs(out, pr);
+                const float Ssum = fmaf(ai.x, ai.x, ai.y * ai.y) + fmaf(aj.x, aj.x, aj.y * aj.y);
+                const float t = fmaf(ai.x, ai.x, ai.y * ai.y) / Ssum;
+                const float lq_rev = log_learned_density(pr, t, argf(ai) + argf(hi2), argf(aj) + argf(hj2)) -
+                                     log_plain_density(t);
+                lq_ratio = lq_rev - lq_fwd;
+                accept = ok && (logf(cu) < -beta * dE + lq_ratio);
+            }
+            if (accept) {
+                E += (double)dE;
+                nacc++;
+            } else {
+                sp[i0 * kRepBlock + lane] = ai;
+                sp[j0 * kRepBlock + lane] = aj;
+            }
+            nprop++;
+            if (L.mode == 1 && accept && active && L.records != nullptr && u01f(g.next()) < L.rec_prob) {
+                float f[kMlpIn];
+                pair_features(ai, aj, hi1, hj1, beta, f);
+                const unsigned long long slot = atomicAdd(L.rec_count, 1ull) % (unsigned long long)L.rec_cap;
+                float* rec = L.records + slot * kRecordFloats;
+                for (int q = 0; q < kMlpIn; q++) rec[q] = f[q];
+                // t' within float range of (0, 1): log t' and log(1-t') stay finite
+                rec[kMlpIn] = fminf(fmaxf(tn, 1e-6f), 1.0f - 1e-6f);
+                rec[kMlpIn + 1] = psi_i;
+                rec[kMlpIn + 2] = psi_j;
+            }
+            if (P.trace != nullptr && U.sample == P.trace_sample && U.rep_begin + lane == P.trace_rep && active) {
+                const long long idx = (sw - P.trace_sweep0) * steps + k;
+                if (idx >= 0 && idx < P.trace_cap) {
+                    pspin_move_record* r = reinterpret_cast<pspin_move_record*>(P.trace) + idx;
+                    r->i0 = i0; r->j0 = j0;
+                    r->ai_old[0] = ai.x; r->ai_old[1] = ai.y; r->aj_old[0] = aj.x; r->aj_old[1] = aj.y;
+                    r->ai_new[0] = ain.x; r->ai_new[1] = ain.y; r->aj_new[0] = ajn.x; r->aj_new[1] = ajn.y;
+                    r->dE = dE;
+                    r->accepted = accept ? 1 : 0;
+                    r->log_q_ratio = lq_ratio;
+                    r->log_u = logf(cu);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (!ok_wait && lane == 0)
+        for (uint32_t q = consumed; q < issued; q++) mbar_wait(bars + q % kStages, (q / kStages) & 1u, P.status);
+    for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
+        const int site = idx >> 5, l = idx & 31;
+        if (l < U.rep_count) P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l] = sp[idx];
+    }
+    if (warp == 0 && active) {
+        P.energy[gr] = E;
+        P.accepted[gr] += nacc;
+        P.proposed[gr] += nprop;
+    }
+}
+
+cudaError_t launch_learned_sweep(const SweepParams& p, const LearnParams& l, int n_units, int max_N,
+                                 cudaStream_t st) {
+    if (n_units <= 0) return cudaSuccess;
+    const size_t smem = learned_smem_bytes(max_N, p.warps);
+    cudaError_t e = cudaFuncSetAttribute(learned_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    learned_sweep_kernel<<<n_units, 32 * p.warps, smem, st>>>(p, l);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ training
+// Per record: forward and backward through the network (FP32 master
+// weights); activations and deltas saved for the per-parameter reduction.
+constexpr int kSaveFloats = kMlpIn + 2 * kMlpHidden + 2 * kMlpHidden + kMlpOut;   // f, h1, h2, d1, d2, d3
+
+__global__ void mlp_fwd_bwd_kernel(const float* __restrict__ w, const float* __restrict__ records,
+                                   const int* __restrict__ index, int n, float* __restrict__ save,
+                                   float* __restrict__ loss) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const float* rec = records + (int64_t)(index ? index[b] : b) * kRecordFloats;
+    float* sv = save + (int64_t)b * kSaveFloats;
+    float* f = sv;
+    float* h1 = f + kMlpIn;
+    float* h2 = h1 + kMlpHidden;
+    float* d1 = h2 + kMlpHidden;
+    float* d2 = d1 + kMlpHidden;
+    float* d3 = d2 + kMlpHidden;
+    for (int i = 0; i < kMlpIn; i++) f[i] = rec[i];
+    float out[kMlpOut];
+    mlp_forward_rows(w, f, h1, h2, out);
+    loss[b] = loss_output_grad(out, rec[kMlpIn], rec[kMlpIn + 1], rec[kMlpIn + 2], d3);
+    for (int i = 0; i < kMlpHidden; i++) {
+        float s = 0.f;
+        for (int o = 0; o < kMlpOut; o++) s = fmaf(w[kOffW3 + o * kMlpHidden + i], d3[o], s);
+        d2[i] = s * (1.0f - h2[i] * h2[i]);
+    }
+    for (int i = 0; i < kMlpHidden; i++) {
+        float s = 0.f;
+        for (int o = 0; o < kMlpHidden; o++) s = fmaf(w[kOffW2 + o * kMlpHidden + i], d2[o], s);
+        d1[i] = s * (1.0f - h1[i] * h1[i]);
+    }
+}
+
+// gradient of the mean loss, one thread per parameter, summed over records
+// in a fixed order (deterministic)
+__global__ void mlp_grad_reduce_kernel(const float* __restrict__ save, int n, float* __restrict__ grad) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kMlpParams) return;
+    // saved layout per record: f | h1 | h2 | d1 | d2 | d3
+    constexpr int F0 = 0, H1 = kMlpIn, H2 = H1 + kMlpHidden, D1 = H2 + kMlpHidden, D2 = D1 + kMlpHidden,
+                  D3 = D2 + kMlpHidden;
+    int dofs, aofs = 0, ai = -1;   // delta index; activation index (ai < 0: bias)
+    if (p < kOffB1) { dofs = D1 + p / kMlpIn; aofs = F0; ai = p % kMlpIn; }
+    else if (p < kOffW2) { dofs = D1 + (p - kOffB1); }
+    else if (p < kOffB2) { const int q = p - kOffW2; dofs = D2 + q / kMlpHidden; aofs = H1; ai = q % kMlpHidden; }
+    else if (p < kOffW3) { dofs = D2 + (p - kOffB2); }
+    else if (p < kOffB3) { const int q = p - kOffW3; dofs = D3 + q / kMlpHidden; aofs = H2; ai = q % kMlpHidden; }
+    else { dofs = D3 + (p - kOffB3); }
+    float s = 0.f;
+    for (int b = 0; b < n; b++) {
+        const float* sv = save + (int64_t)b * kSaveFloats;
+        s = fmaf(sv[dofs], ai >= 0 ? sv[aofs + ai] : 1.0f, s);
+    }
+    grad[p] = s / (float)n;
+}
+
+__global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                            const float* __restrict__ g, __nv_bfloat16* __restrict__ wbf, float lr, float b1,
+                            float b2, float eps, float c1, float c2) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kMlpParams) return;
+    const float gp = g[p];
+    const float mp = b1 * m[p] + (1.0f - b1) * gp, vp = b2 * v[p] + (1.0f - b2) * gp * gp;
+    m[p] = mp;
+    v[p] = vp;
+    const float wp = w[p] - lr * (mp / c1) / (sqrtf(vp / c2) + eps);
+    w[p] = wp;
+    wbf[p] = __float2bfloat16_rn(wp);
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ w, __nv_bfloat16* __restrict__ wbf) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < kMlpParams) wbf[p] = __float2bfloat16_rn(w[p]);
+}
+
+__global__ void sample_index_kernel(int* __restrict__ idx, int n, unsigned long long filled, uint32_t k0, uint32_t k1,
+                                    uint32_t step) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const U4 r = philox4x32_10(U4{(uint32_t)b, step, 0x74726e00u, 0u}, k0, k1);
+    idx[b] = (int)(((uint64_t)r.x * filled) >> 32);
+}
+
+cudaError_t launch_mlp_fwd_bwd(const float* w, const float* records, const int* index, int n, float* save,
+                               float* loss, cudaStream_t st) {
+    mlp_fwd_bwd_kernel<<<(n + 127) / 128, 128, 0, st>>>(w, records, index, n, save, loss);
+    return cudaGetLastError();
+}
+cudaError_t launch_mlp_grad(const float* save, int n, float* grad, cudaStream_t st) {
+    mlp_grad_reduce_kernel<<<(kMlpParams + 255) / 256, 256, 0, st>>>(save, n, grad);
+    return cudaGetLastError();
+}
+cudaError_t launch_adam(float* w, float* m, float* v, const float* g, __nv_bfloat16* wbf, float lr, int t,
+                        cudaStream_t st) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    adam_kernel<<<(kMlpParams + 255) / 256, 256, 0, st>>>(w, m, v, g, wbf, lr, b1, b2, 1e-8f,
+                                                          1.0f - powf(b1, (float)t), 1.0f - powf(b2, (float)t));
+    return cudaGetLastError();
+}
+cudaError_t launch_to_bf16(const float* w, __nv_bfloat16* wbf, cudaStream_t st) {
+    to_bf16_kernel<<<(kMlpParams + 255) / 256, 256, 0, st>>>(w, wbf);
+    return cudaGetLastError();
+}
+cudaError_t launch_sample_index(int* idx, int n, unsigned long long filled, uint64_t key, uint32_t step,
+                                cudaStream_t st) {
+    sample_index_kernel<<<(n + 255) / 256, 256, 0, st>>>(idx, n, filled, (uint32_t)key, (uint32_t)(key >> 32), step);
+    return cudaGetLastError();
+}
+
+}  // namespace pspin

@@ -1,0 +1,255 @@
+// mlp.cuh -- the learned pair-move proposal: a small MLP over the pair's
+// local-field features that outputs a Beta law for the amplitude transfer
+// t' = |a_i'|^2 / (|a_i|^2 + |a_j|^2) and one 4-component von Mises mixture
+// per site for the new phase measured from the site's field,
+// psi = theta' + arg(h).  Densities, samplers and the loss gradient.
+//
+// Plain move (spins.h:17-52) in the same coordinates: t' ~ Beta(1/2, 1/2)
+// (t' = cos^2 alpha, alpha uniform) and uniform phases, independent of the
+// state.  The plain chain with acceptance min(1, e^{-beta dE}) samples
+// e^{-beta E} nu with nu ~ Beta(1/2,1/2)(t) (the measure its proposal is
+// symmetric for); a learned proposal keeps that target with
+//   A = min(1, e^{-beta dE} [q_L(x|x')/q_P(x|x')] / [q_L(x'|x)/q_P(x'|x)]).
+#pragma once
+#include <cuda_bf16.h>
+#include <cstdint>
+#include "rng.cuh"
+
+namespace pspin {
+
+constexpr int kMlpIn = 8, kMlpHidden = 64, kMlpOut = 26;
+constexpr int kOffW1 = 0;
+constexpr int kOffB1 = kOffW1 + kMlpHidden * kMlpIn;
+constexpr int kOffW2 = kOffB1 + kMlpHidden;
+constexpr int kOffB2 = kOffW2 + kMlpHidden * kMlpHidden;
+constexpr int kOffW3 = kOffB2 + kMlpHidden;
+constexpr int kOffB3 = kOffW3 + kMlpOut * kMlpHidden;
+constexpr int kMlpParams = kOffB3 + kMlpOut;                 // 6426
+constexpr int kRecordFloats = kMlpIn + 3;                    // features, t', psi_i, psi_j
+constexpr float kKappaMax = 50.0f;
+constexpr float kTwoPi = 6.283185307179586f;
+
+// Features of a pair at one state: log(1+beta sqrt(S)|h|) for both sites,
+// cos/sin of each site's phase measured from its field, 2t-1, log(beta).
+__device__ __forceinline__ void pair_features(float2 ai, float2 aj, float2 hi, float2 hj, float beta, float* f) {
+    const float ri = fmaf(ai.x, ai.x, ai.y * ai.y), rj = fmaf(aj.x, aj.x, aj.y * aj.y);
+    const float S = ri + rj, sS = sqrtf(S);
+    const float mi = sqrtf(fmaf(hi.x, hi.x, hi.y * hi.y)), mj = sqrtf(fmaf(hj.x, hj.x, hj.y * hj.y));
+    f[0] = log1pf(beta * sS * mi);
+    f[1] = log1pf(beta * sS * mj);
+    const float pi = atan2f(ai.y, ai.x) + atan2f(hi.y, hi.x);
+    const float pj = atan2f(aj.y, aj.x) + atan2f(hj.y, hj.x);
+    float s, c;
+    sincosf(pi, &s, &c);
+    f[2] = c; f[3] = s;
+    sincosf(pj, &s, &c);
+    f[4] = c; f[5] = s;
+    f[6] = 2.0f * ri / S - 1.0f;
+    f[7] = logf(beta > 1e-30f ? beta : 1e-30f);
+}
+
+// Forward pass of one record with FP32 weights; the hidden activations go to
+// the record's rows h1[64], h2[64] (which the backward pass reads) and are
+// read back from there.  (A variant holding them in per-thread arrays gave
+// wrong outputs for the second site's mixture under nvcc 12.9 -O3; this form
+// is checked against float64 autograd.)
+__device__ __forceinline__ void mlp_forward_rows(const float* __restrict__ w, const float* f, float* h1, float* h2,
+                                                 float* out) {
+    for (int o = 0; o < kMlpHidden; o++) {
+        float z = w[kOffB1 + o];
+#pragma unroll
+        for (int i = 0; i < kMlpIn; i++) z = fmaf(w[kOffW1 + o * kMlpIn + i], f[i], z);
+        h1[o] = tanhf(z);
+    }
+    for (int o = 0; o < kMlpHidden; o++) {
+        float z = w[kOffB2 + o];
+        for (int i = 0; i < kMlpHidden; i++) z = fmaf(w[kOffW2 + o * kMlpHidden + i], h1[i], z);
+        h2[o] = tanhf(z);
+    }
+    for (int o = 0; o < kMlpOut; o++) {
+        float z = w[kOffB3 + o];
+        for (int i = 0; i < kMlpHidden; i++) z = fmaf(w[kOffW3 + o * kMlpHidden + i], h2[i], z);
+        out[o] = z;
+    }
+}
+
+__device__ __forceinline__ float softplusf(float x) { return x > 20.f ? x : log1pf(expf(x)); }
+__device__ __forceinline__ float sigmoidf(float x) { return 1.0f / (1.0f + expf(-x)); }
+
+struct ProposalParams {
+    float a, b;               // Beta(a, b) for t'
+    float w[2][4], mu[2][4], kappa[2][4];   // mixtures for psi_i, psi_j
+};
+
+__device__ __forceinline__ void decode_outputs(const float* o, ProposalParams& p) {
+    p.a = 0.05f + softplusf(o[0]);
+    p.b = 0.05f + softplusf(o[1]);
+    for (int s = 0; s < 2; s++) {
+        const float* q = o + 2 + 12 * s;
+        float m = q[0];
+        for (int k = 1; k < 4; k++) m = fmaxf(m, q[k]);
+        float z = 0.f;
+        for (int k = 0; k < 4; k++) { p.w[s][k] = expf(q[k] - m); z += p.w[s][k]; }
+        for (int k = 0; k < 4; k++) {
+            p.w[s][k] /= z;
+            p.mu[s][k] = q[4 + k];
+            p.kappa[s][k] = kKappaMax * sigmoidf(q[8 + k]) + 0.01f;
+        }
+    }
+}
+
+// log I0(k) for 0 < k <= kKappaMax (CUDA's Bessel function, no overflow there)
+__device__ __forceinline__ float log_i0f(float k) { return logf(cyl_bessel_i0f(k)); }
+
+__device__ __forceinline__ float log_beta_pdf(float t, float a, float b) {
+    return (a - 1.0f) * logf(t) + (b - 1.0f) * log1pf(-t) - (lgammaf(a) + lgammaf(b) - lgammaf(a + b));
+}
+
+// log of the plain proposal density in (t', theta_i', theta_j'):
+// Beta(1/2,1/2)(t) / (2 pi)^2
+__device__ __forceinline__ float log_plain_density(float t) {
+    return -0.5f * logf(t) - 0.5f * log1pf(-t) - 1.1447298858494002f - 2.0f * 1.8378770664093453f;
+}
+
+__device__ __forceinline__ float log_vm_mix(const ProposalParams& p, int s, float psi) {
+    float m = -1e30f, v[4];
+    for (int k = 0; k < 4; k++) {
+        v[k] = logf(p.w[s][k]) + p.kappa[s][k] * cosf(psi - p.mu[s][k]) - 1.8378770664093453f - log_i0f(p.kappa[s][k]);
+        m = fmaxf(m, v[k]);
+    }
+    float z = 0.f;
+    for (int k = 0; k < 4; k++) z += expf(v[k] - m);
+    return m + logf(z);
+}
+
+__device__ __forceinline__ float log_learned_density(const ProposalParams& p, float t, float psi_i, float psi_j) {
+    return log_beta_pdf(t, p.a, p.b) + log_vm_mix(p, 0, psi_i) + log_vm_mix(p, 1, psi_j);
+}
+
+// ------------------------------------------------------------------ sampling
+// A counter-based stream of uniforms for one replica's move: Philox blocks
+// (key, {step, sweep, tag + n}) drawn four words at a time.
+struct MoveStream {
+    uint32_t k0, k1, step, sw_lo, sw_hi, n, used;
+    U4 w;
+    __device__ __forceinline__ uint32_t next() {
+        if (used == 4) {
+            w = philox4x32_10(U4{step, sw_lo, sw_hi, 0x6c726e00u + n}, k0, k1);
+            n++;
+            used = 0;
+        }
+        const uint32_t v = used == 0 ? w.x : used == 1 ? w.y : used == 2 ? w.z : w.w;
+        used++;
+        return v;
+    }
+    __device__ __forceinline__ float uniform() { return u01f_open0(next()); }   // (0, 1]
+};
+
+__device__ __forceinline__ float normal(MoveStream& g) {
+    const float u1 = g.uniform(), u2 = g.uniform();
+    return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+}
+
+// Marsaglia & Tsang (2000) gamma sampler, bounded; returns < 0 on exhaustion
+__device__ __forceinline__ float gamma_sample(MoveStream& g, float a) {
+    float boost = 1.0f;
+    if (a < 1.0f) {
+        boost = powf(g.uniform(), 1.0f / a);
+        a += 1.0f;
+    }
+    const float d = a - 1.0f / 3.0f, c = rsqrtf(9.0f * d);
+    for (int it = 0; it < 32; it++) {
+        const float x = normal(g);
+        float v = 1.0f + c * x;
+        if (v <= 0.0f) continue;
+        v = v * v * v;
+        const float u = g.uniform();
+        if (logf(u) < 0.5f * x * x + d - d * v + d * logf(v)) return d * v * boost;
+    }
+    return -1.0f;
+}
+
+// Best & Fisher (1979) von Mises sampler around 0, bounded; -10 on exhaustion
+__device__ __forceinline__ float vonmises_sample(MoveStream& g, float kappa) {
+    if (kappa < 1e-3f) return kTwoPi * g.uniform() - 3.14159265f;
+    const float tau = 1.0f + sqrtf(1.0f + 4.0f * kappa * kappa);
+    const float rho = (tau - sqrtf(2.0f * tau)) / (2.0f * kappa);
+    const float r = (1.0f + rho * rho) / (2.0f * rho);
+    for (int it = 0; it < 32; it++) {
+        const float u1 = g.uniform(), u2 = g.uniform();
+        const float z = cospif(u1);
+        const float f = (1.0f + r * z) / (r + z);
+        const float c = kappa * (r - f);
+        if (c * (2.0f - c) - u2 > 0.0f || logf(c / u2) + 1.0f - c >= 0.0f) {
+            const float th = acosf(fminf(1.0f, fmaxf(-1.0f, f)));
+            return g.uniform() < 0.5f ? -th : th;
+        }
+    }
+    return -10.0f;
+}
+
+// returns false when a bounded sampler ran out (the move is then rejected)
+__device__ __forceinline__ bool sample_move(MoveStream& g, const ProposalParams& p, float& t, float& psi_i,
+                                            float& psi_j) {
+    const float x = gamma_sample(g, p.a), y = gamma_sample(g, p.b);
+    if (x < 0.f || y < 0.f || x + y <= 0.f) return false;
+    t = x / (x + y);
+    if (!(t > 1e-7f && t < 1.0f - 1e-7f)) return false;
+    float psi[2];
+    for (int s = 0; s < 2; s++) {
+        const float u = g.uniform();
+        int k = 0;
+        float acc = p.w[s][0];
+        while (k < 3 && u > acc) { k++; acc += p.w[s][k]; }
+        const float v = vonmises_sample(g, p.kappa[s][k]);
+        if (v < -9.0f) return false;
+        psi[s] = p.mu[s][k] + v;
+    }
+    psi_i = psi[0];
+    psi_j = psi[1];
+    return true;
+}
+
+// ------------------------------------------------------------------ training
+// digamma by recurrence to x >= 6 and the asymptotic series
+// (Abramowitz & Stegun 6.3.18)
+__device__ __forceinline__ float digammaf_series(float x) {
+    float r = 0.f;
+    while (x < 6.0f) { r -= 1.0f / x; x += 1.0f; }
+    const float i2 = 1.0f / (x * x);
+    return r + logf(x) - 0.5f / x - i2 * (1.0f / 12.0f - i2 * (1.0f / 120.0f - i2 / 252.0f));
+}
+
+// d(-log q_L)/d(outputs) for one record; returns -log q_L
+__device__ __forceinline__ float loss_output_grad(const float* o, float t, float psi_i, float psi_j, float* g) {
+    ProposalParams p;
+    decode_outputs(o, p);
+    float loss = -log_learned_density(p, t, psi_i, psi_j);
+    const float dab = digammaf_series(p.a + p.b);
+    g[0] = -(logf(t) - digammaf_series(p.a) + dab) * sigmoidf(o[0]);
+    g[1] = -(log1pf(-t) - digammaf_series(p.b) + dab) * sigmoidf(o[1]);
+    const float psis[2] = {psi_i, psi_j};
+    for (int s = 0; s < 2; s++) {
+        const float* q = o + 2 + 12 * s;
+        float* gq = g + 2 + 12 * s;
+        float v[4], m = -1e30f;
+        for (int k = 0; k < 4; k++) {
+            v[k] = logf(p.w[s][k]) + p.kappa[s][k] * cosf(psis[s] - p.mu[s][k]) - log_i0f(p.kappa[s][k]);
+            m = fmaxf(m, v[k]);
+        }
+        float z = 0.f;
+        for (int k = 0; k < 4; k++) { v[k] = expf(v[k] - m); z += v[k]; }
+        for (int k = 0; k < 4; k++) {
+            const float rk = v[k] / z;          // responsibility
+            const float kap = p.kappa[s][k], dpsi = psis[s] - p.mu[s][k];
+            gq[k] = p.w[s][k] - rk;
+            gq[4 + k] = -rk * kap * sinf(dpsi);
+            const float ratio = cyl_bessel_i1f(kap) / cyl_bessel_i0f(kap);
+            const float sg = sigmoidf(q[8 + k]);
+            gq[8 + k] = -rk * (cosf(dpsi) - ratio) * kKappaMax * sg * (1.0f - sg);
+        }
+    }
+    return loss;
+}
+
+}  // namespace pspin

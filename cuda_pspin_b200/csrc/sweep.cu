@@ -25,208 +25,10 @@
 //  * The lists reach shared memory through per-warp TMA (cp.async.bulk)
 //    rings that prefetch across moves, so no warp waits on L2 latency.
 //  * FP32 amplitudes and fields; the running energy is FP64.
-#include "internal.h"
-#include "rng.cuh"
+#include "sweep_common.cuh"
 #include "../../include/pspin.h"
 
 namespace pspin {
-
-template <int VARIANT>
-__device__ __forceinline__ void propose(float2 ai, float2 aj, U4 w, float2& ain, float2& ajn) {
-    if (VARIANT == 0) {
-        // spins.h:17-52: a_i' = a_i e^{-i phi1} sqrt((r1+r2)/r1) cos(alpha),
-        //                a_j' = a_j e^{-i phi2} sqrt((r1+r2)/r2) sin(alpha)
-        float r1 = fmaf(ai.x, ai.x, ai.y * ai.y);
-        float r2 = fmaf(aj.x, aj.x, aj.y * aj.y);
-        float sa, ca, s1, c1, s2, c2;
-        sincospif(2.0f * u01f(w.x), &sa, &ca);
-        sincospif(2.0f * u01f(w.y), &s1, &c1);
-        sincospif(2.0f * u01f(w.z), &s2, &c2);
-        float s = r1 + r2;
-        float f1 = sqrtf(s / r1) * ca;
-        float f2 = sqrtf(s / r2) * sa;
-        ain = make_float2(fmaf(ai.x, c1, ai.y * s1) * f1, fmaf(ai.y, c1, -ai.x * s1) * f1);
-        ajn = make_float2(fmaf(aj.x, c2, aj.y * s2) * f2, fmaf(aj.y, c2, -aj.x * s2) * f2);
-    } else {
-        // spins_sparse.h:26-56: |a_i'|^2 = sqrt(S4) sqrt(1-u), |a_j'|^2 = sqrt(S4) sqrt(u),
-        // absolute phases phi1, phi2
-        float u = u01f_open0(w.x);
-        float r1 = fmaf(ai.x, ai.x, ai.y * ai.y);
-        float r2 = fmaf(aj.x, aj.x, aj.y * aj.y);
-        float q = sqrtf(fmaf(r1, r1, r2 * r2));
-        float m1 = sqrtf(q * sqrtf(1.0f - u));
-        float m2 = sqrtf(q * sqrtf(u));
-        float s1, c1, s2, c2;
-        sincospif(2.0f * u01f(w.y), &s1, &c1);
-        sincospif(2.0f * u01f(w.z), &s2, &c2);
-        ain = make_float2(m1 * c1, m1 * s1);
-        ajn = make_float2(m2 * c2, m2 * s2);
-    }
-}
-
-// ---------------------------------------------------------------- TMA ring
-// Each warp streams the chunks of its share of the two site lists of every
-// move through a ring of kStages shared-memory slots.  Lane 0 issues 1-D
-// bulk copies (cp.async.bulk, completion counted on one mbarrier per slot)
-// kStages-1 chunks ahead of the chunk being read; the pair schedule is known
-// in advance, so the prefetch runs across move boundaries.  Waits are
-// bounded: after ~2^31 clocks the kernel sets *status and stops waiting.
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-__device__ __forceinline__ void fence_async_shared() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// bounded wait; returns false (and raises the status word) on time-out
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > (1ll << 31)) {
-            atomicOr(status, 1);
-            return false;
-        }
-    }
-    return true;
-}
-
-// Position in a warp's chunk stream: move m, list (0: site i0, 1: site j0),
-// chunk c of [c, c_end).
-struct Cursor {
-    int m, which, c, c_end;
-};
-
-struct Stream {
-    uint32_t key0, key1;
-    int N;
-    const int* site_chunks;   // this sample's N*(kSplit+1) absolute chunk indices
-    long long sweep0;
-    int steps, total, part0, part1;
-
-    __device__ __forceinline__ void range(int m, int which, int& c, int& c_end) const {
-        int i0, j0;
-        const long long sw = sweep0 + m / steps;
-        pair_pick(key0, key1, (uint64_t)sw, (uint32_t)(m % steps), N, i0, j0);
-        const int* sc = site_chunks + (which ? j0 : i0) * (kSplit + 1);
-        c = __ldg(sc + part0);
-        c_end = __ldg(sc + part1);
-    }
-    // move to the next chunk (skipping empty ranges); m == total at the end
-    __device__ __forceinline__ void next(Cursor& k) const {
-        k.c++;
-        while (k.c >= k.c_end) {
-            if (++k.which == 2) {
-                k.which = 0;
-                if (++k.m >= total) return;
-            }
-            range(k.m, k.which, k.c, k.c_end);
-        }
-    }
-    __device__ __forceinline__ Cursor first() const {
-        Cursor k{0, 0, 0, 0};
-        if (total <= 0) return k;
-        range(0, 0, k.c, k.c_end);
-        k.c--;
-        next(k);
-        return k;
-    }
-};
-
-// Field contribution of the groups in one staged chunk for this lane's replica.
-__device__ __forceinline__ void accumulate_chunk(const int2* __restrict__ R, int n,
-                                                 const float2* __restrict__ sp, int lane,
-                                                 float& hx, float& hy) {
-    int e = 0;
-    while (e < n) {
-        const int2 h = R[e];
-        const int len = h.x;
-        const int p = h.y >> 16, o1 = h.y & 0xFFFF;
-        const float2 ap = sp[p * kRepBlock + lane];
-        const float2 ao = sp[o1 * kRepBlock + lane];
-        // a_p * conj(a_o1)
-        const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
-        const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
-        float yx = 0.f, yy = 0.f;
-        const int2* __restrict__ d = R + e + 1;
-#pragma unroll 4
-        for (int t = 0; t < len; t++) {
-            const int2 v = d[t];
-            const float g = __int_as_float(v.x);
-            const float2 a = sp[v.y * kRepBlock + lane];
-            yx = fmaf(g, a.x, yx);       // Y += g conj(a_o2)
-            yy = fmaf(-g, a.y, yy);
-        }
-        hx = fmaf(px, yx, fmaf(-py, yy, hx));
-        hy = fmaf(px, yy, fmaf(py, yx, hy));
-        e += len + 1;
-    }
-}
-
-// Field contribution of the fully connected tiles in one staged chunk
-// (16-byte records: header, then rows of 4 couplings).  One gathered
-// a_inner feeds four partners: 8 FFMA per shared-memory gather.
-__device__ __forceinline__ void accumulate_tiles(const int2* __restrict__ R2, int n,
-                                                 const float2* __restrict__ sp, int lane,
-                                                 float& hx, float& hy) {
-    const int4* __restrict__ R = reinterpret_cast<const int4*>(R2);
-    const int n16 = n >> 1;
-    int e = 0;
-    while (e < n16) {
-        const int4 hd = R[e];
-        const int outer = hd.x & 0xFFFF, lo = hd.x >> 16, hi = hd.y;
-        const float2 ao = sp[outer * kRepBlock + lane];
-        float y0x = 0.f, y0y = 0.f, y1x = 0.f, y1y = 0.f, y2x = 0.f, y2y = 0.f, y3x = 0.f, y3y = 0.f;
-        const float4* __restrict__ C = reinterpret_cast<const float4*>(R + e + 1);
-        const float2* __restrict__ A = sp + lo * kRepBlock + lane;
-        const int len = hi - lo;
-#pragma unroll 2
-        for (int t = 0; t < len; t++) {
-            const float4 c = C[t];
-            const float2 a = A[t * kRepBlock];
-            y0x = fmaf(c.x, a.x, y0x); y0y = fmaf(-c.x, a.y, y0y);
-            y1x = fmaf(c.y, a.x, y1x); y1y = fmaf(-c.y, a.y, y1y);
-            y2x = fmaf(c.z, a.x, y2x); y2y = fmaf(-c.z, a.y, y2y);
-            y3x = fmaf(c.w, a.x, y3x); y3y = fmaf(-c.w, a.y, y3y);
-        }
-        // h += sum_k a_pk conj(a_outer) Y_k
-        const int pk[4] = {hd.z & 0xFFFF, hd.z >> 16, hd.w & 0xFFFF, hd.w >> 16};
-        const float yx[4] = {y0x, y1x, y2x, y3x}, yy[4] = {y0y, y1y, y2y, y3y};
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const float2 ap = sp[pk[k] * kRepBlock + lane];
-            const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
-            const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
-            hx = fmaf(px, yx[k], fmaf(-py, yy[k], hx));
-            hy = fmaf(px, yy[k], fmaf(py, yx[k], hy));
-        }
-        e += 1 + len;
-    }
-}
 
 template <int VARIANT>
 __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepParams P) {
@@ -383,6 +185,8 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepParams P) {
                     rec->aj_new[0] = cajn.x; rec->aj_new[1] = cajn.y;
                     rec->dE = dE;
                     rec->accepted = accept ? 1 : 0;
+                    rec->log_q_ratio = 0.f;
+                    rec->log_u = logf(cu);
                 }
             }
             if (m + 1 < total) prepare(m + 1);

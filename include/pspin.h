@@ -100,6 +100,8 @@ typedef struct pspin_move_record {
     float ai_new[2], aj_new[2];
     float dE;                /* FP32 dE the kernel accepted or rejected on */
     int32_t accepted;
+    float log_q_ratio;       /* log[q(x|x')/q(x'|x)] relative to the plain move (0 for it) */
+    float log_u;             /* log of the uniform the decision compared against */
 } pspin_move_record;
 
 typedef struct pspin_state pspin_state;
@@ -163,6 +165,29 @@ enum { PSPIN_FIELDS_FP64 = 0,      /* FP64 sum over the quartet table */
  * tensor-core method builds the symmetric pair-space coupling matrix on its
  * first call for the sample (C(N,2)^2 BF16 x 3 on the device). */
 int  pspin_local_fields(pspin_state* s, int sample, int method, double* h, double* energy);
+
+/* ---- learned pair proposal (no reference counterpart) ----------------- */
+/* Proposal used by pspin_sweep / pspin_pt_run (dense variant):
+ *   PLAIN         the reference's move (spins.h:17-52), one field pass;
+ *   PLAIN_FIELDS  the same move with fields at both ends of every move and,
+ *                 after pspin_learn_init, accepted moves recorded for training;
+ *   LEARNED       the network's move, accepted with the exact MH ratio
+ *                 min(1, e^{-beta dE} [q_L(x|x')/q_P(x|x')]/[q_L(x'|x)/q_P(x'|x)]),
+ *                 so the stationary law is the plain chain's. */
+enum { PSPIN_PROPOSAL_PLAIN = 0, PSPIN_PROPOSAL_PLAIN_FIELDS = 1, PSPIN_PROPOSAL_LEARNED = 2 };
+int  pspin_set_proposal(pspin_state* s, int proposal);
+/* Network 8 -> 64 -> 64 -> 26 (tanh), Xavier-initialised from seed; a ring of
+ * `capacity` training records (features[8], t', psi_i, psi_j), each accepted
+ * PLAIN_FIELDS move being recorded with probability record_prob. */
+int  pspin_learn_init(pspin_state* s, uint64_t seed, int capacity, float record_prob);
+int  pspin_learn_params(pspin_state* s, float* get /*[6426] or NULL*/, const float* set /*or NULL*/);
+/* `steps` Adam steps on minibatches of `batch` records drawn from the ring;
+ * mean_loss: mean -log q_L of the last minibatch. */
+int  pspin_learn_train(pspin_state* s, int steps, int batch, float lr, double* mean_loss);
+int  pspin_learn_records(pspin_state* s, int64_t* n_recorded, float* out /*[max][11] or NULL*/, int max);
+/* Loss and gradient of the mean -log q_L over n host records (FP32
+ * weights): the check of the backward pass. */
+int  pspin_learn_loss_grad(pspin_state* s, const float* records, int n, double* loss, float* grad);
 
 /* ---- per-move trace (tests) ------------------------------------------ */
 int  pspin_trace_get(pspin_state* s, pspin_move_record* out, int max_records, int* n_records);

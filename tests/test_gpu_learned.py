@@ -1,0 +1,263 @@
+"""The learned pair proposal.
+
+* its training gradient (own backward kernels, FP32) equals a float64 torch
+  autograd evaluation of the same loss (-log q_L of recorded moves);
+* with any network the chain keeps the plain chain's stationary law: at
+  beta = 0 the plain move samples |a_k|^2/R ~ Dirichlet(1/2,...,1/2) (not the
+  uniform sphere's Dirichlet(1)), and so must the learned move with its MH
+  correction;
+* every traced learned move's FP32 dE matches the FP64 oracle difference;
+* every learned move's log proposal ratio log[q_L(x|x')/q_P] - log[q_L(x'|x)/q_P]
+  equals a float64 recomputation from the replayed states (fields by exact
+  finite differences of the FP64 energy, which is affine in each site), and
+  each accept decision is log u < -beta dE + that ratio;
+* training on recorded accepted plain moves lowers the loss.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+H, IN, OUT = 64, 8, 26
+
+
+def torch_loss(w, rec):
+    import torch
+    W = torch.tensor(w, dtype=torch.float64, requires_grad=True)
+    r = torch.tensor(rec, dtype=torch.float64)
+    o1 = IN * H
+    W1 = W[:o1].view(H, IN); b1 = W[o1:o1 + H]
+    o2 = o1 + H
+    W2 = W[o2:o2 + H * H].view(H, H); b2 = W[o2 + H * H:o2 + H * H + H]
+    o3 = o2 + H * H + H
+    W3 = W[o3:o3 + OUT * H].view(OUT, H); b3 = W[o3 + OUT * H:]
+    f = r[:, :IN]
+    h1 = torch.tanh(f @ W1.T + b1)
+    h2 = torch.tanh(h1 @ W2.T + b2)
+    o = h2 @ W3.T + b3
+    a = 0.05 + torch.nn.functional.softplus(o[:, 0])
+    b = 0.05 + torch.nn.functional.softplus(o[:, 1])
+    t, pi_, pj_ = r[:, IN], r[:, IN + 1], r[:, IN + 2]
+    lb = (a - 1) * torch.log(t) + (b - 1) * torch.log1p(-t) - (torch.lgamma(a) + torch.lgamma(b) - torch.lgamma(a + b))
+    total = lb
+    for s_, psi in ((0, pi_), (1, pj_)):
+        q = o[:, 2 + 12 * s_: 14 + 12 * s_]
+        logw = torch.log_softmax(q[:, :4], dim=1)
+        mu = q[:, 4:8]
+        kap = 50.0 * torch.sigmoid(q[:, 8:12]) + 0.01
+        comp = logw + kap * torch.cos(psi[:, None] - mu) - np.log(2 * np.pi) - torch.log(torch.special.i0(kap))
+        total = total + torch.logsumexp(comp, dim=1)
+    loss = -total.mean()
+    loss.backward()
+    return loss.item(), W.grad.numpy()
+
+
+def bf16(x):
+    """float32 -> bfloat16 (round to nearest even), returned as float64."""
+    u = np.asarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32).astype(np.float64)
+
+
+def net(w, f):
+    W1 = w[:512].reshape(H, IN); b1 = w[512:576]; W2 = w[576:4672].reshape(H, H); b2 = w[4672:4736]
+    W3 = w[4736:6400].reshape(OUT, H); b3 = w[6400:]
+    return W3 @ np.tanh(W2 @ np.tanh(W1 @ f + b1) + b2) + b3
+
+
+def features(ai, aj, hi, hj, beta):
+    S = abs(ai) ** 2 + abs(aj) ** 2
+    pi, pj = np.angle(ai) + np.angle(hi), np.angle(aj) + np.angle(hj)
+    return np.array([np.log1p(beta * np.sqrt(S) * abs(hi)), np.log1p(beta * np.sqrt(S) * abs(hj)),
+                     np.cos(pi), np.sin(pi), np.cos(pj), np.sin(pj), 2 * abs(ai) ** 2 / S - 1,
+                     np.log(max(beta, 1e-30))])
+
+
+def log_q_over_plain(o, t, psi_i, psi_j):
+    from scipy.special import gammaln, i0, logsumexp
+    sp = lambda x: np.logaddexp(0.0, x)
+    a, b = 0.05 + sp(o[0]), 0.05 + sp(o[1])
+    L = (a - 1) * np.log(t) + (b - 1) * np.log1p(-t) - (gammaln(a) + gammaln(b) - gammaln(a + b))
+    for s_, psi in ((0, psi_i), (1, psi_j)):
+        q = o[2 + 12 * s_:14 + 12 * s_]
+        lw = q[:4] - logsumexp(q[:4])
+        kap = 50.0 / (1.0 + np.exp(-q[8:12])) + 0.01
+        L += logsumexp(lw + kap * np.cos(psi - q[4:8]) - np.log(2 * np.pi) - np.log(i0(kap)))
+    plain = -0.5 * np.log(t) - 0.5 * np.log1p(-t) - np.log(np.pi) - 2 * np.log(2 * np.pi)
+    return L - plain
+
+
+def site_field(ref, s, m):
+    """h_m with E = -Re[a_m h_m] + (terms without a_m): exact finite differences."""
+    z = s.copy()
+    z[m] = 0.0
+    e0 = sum(ref.energy(z))
+    z[m] = 1.0
+    e1 = sum(ref.energy(z))
+    z[m] = 1j
+    e2 = sum(ref.energy(z))
+    return complex(-(e1 - e0), e2 - e0)
+
+
+def _engine(ps, N=8, nrep=8, seed=3, fmc=0):
+    c = ps.default_config(N=N, nrep=nrep, seed=seed, fmc_mode=fmc)
+    return ps.Engine(c, ps.PSPIN_DENSE, ps.make_options(trace=(0, 1, 4096), resync_every=-1))
+
+
+def test_gradient_matches_autograd(ps):
+    rng = np.random.default_rng(0)
+    with _engine(ps) as eng:
+        eng.learn_init(seed=11, capacity=1024)
+        w = eng.learn_params()
+        w = w + rng.normal(0, 0.05, size=w.shape).astype(np.float32)
+        eng.learn_params(w)
+        rec = np.zeros((256, 11), np.float32)
+        rec[:, :IN] = rng.normal(0, 1, (256, IN))
+        rec[:, IN] = rng.uniform(0.02, 0.98, 256)
+        rec[:, IN + 1:] = rng.uniform(-3.1, 3.1, (256, 2))
+        loss_g, grad_g = eng.learn_loss_grad(rec)
+    loss_t, grad_t = torch_loss(w.astype(np.float64), rec.astype(np.float64))
+    assert abs(loss_g - loss_t) < 1e-4 * max(1.0, abs(loss_t))
+    scale = np.abs(grad_t).max()
+    assert np.abs(grad_g - grad_t).max() < 2e-3 * scale, np.abs(grad_g - grad_t).max() / scale
+
+
+def test_learned_chain_keeps_plain_stationary_law_at_beta0(ps):
+    """Dirichlet(1/2) marginals: Var(|a_k|^2/R) = (1/2)(N/2-1/2)/((N/2)^2 (N/2+1))."""
+    N, R = 8, 64
+    c = ps.default_config(N=N, nrep=R, seed=21, fmc_mode=0)
+    out = {}
+    for prop in (ps.PROPOSAL_PLAIN, ps.PROPOSAL_LEARNED):
+        with ps.Engine(c, ps.PSPIN_DENSE, ps.make_options(resync_every=-1)) as eng:
+            eng.learn_init(seed=5, capacity=16)
+            rng = np.random.default_rng(1)
+            w = eng.learn_params()
+            eng.learn_params(w + rng.normal(0, 0.1, w.shape).astype(np.float32))   # an arbitrary network
+            eng.set_proposal(prop)
+            eng.fill_betas(0.0)
+            eng.sweep(200)
+            x = []
+            for _ in range(300):
+                eng.sweep(5)
+                sp = eng.get_spins()[0]
+                r2 = np.abs(sp) ** 2
+                x.append(r2 / r2.sum(axis=1, keepdims=True))
+            x = np.array(x)                                  # [samples, R, N]
+            out[prop] = (x.var(), x.reshape(len(x), -1).var(axis=1).std() / np.sqrt(len(x)))
+            E, acc, prop_ = eng.get_results()
+            if prop == ps.PROPOSAL_LEARNED:
+                assert 0.0 < acc.sum() / prop_.sum() < 1.0
+    a0, ai = N / 2, 0.5
+    dirichlet_half = ai * (a0 - ai) / (a0 * a0 * (a0 + 1))
+    dirichlet_one = 1.0 * (N - 1.0) / (N * N * (N + 1))
+    for prop, (v, se) in out.items():
+        print(prop, v, dirichlet_half, dirichlet_one)
+        assert abs(v - dirichlet_half) < 0.05 * dirichlet_half
+        assert abs(v - dirichlet_one) > 0.2 * dirichlet_one
+
+
+@pytest.mark.parametrize("proposal", [1, 2])
+@pytest.mark.parametrize("kw", [dict(N=12, nrep=4, fmc_mode=2, seed=7), dict(N=16, nrep=8, fmc_mode=0, seed=5)])
+def test_two_pass_moves_dE_against_fp64(ps, orc, kw, proposal):
+    """PLAIN_FIELDS and LEARNED moves evaluate dE from two field passes."""
+    c = ps.default_config(**kw)
+    if c.fmc_mode > 0 and c.gamma <= 0.0:
+        c.gamma = 1.0 / (2.0 * (c.N - 1))
+    ref = orc.DenseInit(orc.cfg(**kw))
+    N, rep, nsw = c.N, 1, 10
+    cap = nsw * (N // 2)
+    with ps.Engine(c, ps.PSPIN_DENSE, ps.make_options(trace=(0, rep, cap), resync_every=-1)) as eng:
+        eng.learn_init(seed=3, capacity=16)
+        eng.set_proposal(proposal)
+        s0 = eng.get_spins()[0][rep].copy()
+        eng.fill_betas(1.0 / 0.7)
+        eng.sweep(nsw)
+        tr = eng.trace(cap)
+        E, acc, prop = eng.get_results()
+    assert len(tr) == cap
+    worst, _, n = orc.check_trace(ref, s0, tr)
+    assert worst <= 1e-5, worst
+    assert 0 < acc[rep] <= prop[rep]
+
+
+def test_learned_moves_mh_ratio_against_float64(ps, orc):
+    kw = dict(N=12, nrep=4, fmc_mode=2, seed=7)
+    c = ps.default_config(**kw)
+    c.gamma = 1.0 / (2.0 * (c.N - 1))
+    ref = orc.DenseInit(orc.cfg(**kw))
+    T, rep, nsw = 0.7, 2, 8
+    cap = nsw * (c.N // 2)
+    rng = np.random.default_rng(4)
+    with ps.Engine(c, ps.PSPIN_DENSE, ps.make_options(trace=(0, rep, cap), resync_every=-1)) as eng:
+        eng.learn_init(seed=8, capacity=16)
+        w = eng.learn_params()
+        w = eng.learn_params(w + rng.normal(0, 0.1, w.shape).astype(np.float32))
+        eng.set_proposal(ps.PROPOSAL_LEARNED)
+        s = eng.get_spins()[0][rep].astype(np.complex64).astype(np.complex128)
+        eng.fill_betas(1.0 / T)
+        eng.sweep(nsw)
+        tr = eng.trace(cap)
+    wb = bf16(w)
+    beta = np.float32(1.0 / T)
+    checked, worst = 0, 0.0
+    for r in tr:
+        i, j = int(r["i0"]), int(r["j0"])
+        ai, aj = complex(*r["ai_old"]), complex(*r["aj_old"])
+        ain, ajn = complex(*r["ai_new"]), complex(*r["aj_new"])
+        assert s[i] == ai and s[j] == aj
+        # the decision is the recorded comparison
+        assert bool(r["accepted"]) == bool(r["log_u"] < np.float32(-beta * r["dE"]) + r["log_q_ratio"])
+        if ain != ai or ajn != aj:
+            x1 = s.copy()
+            x1[i], x1[j] = ain, ajn
+            hi1, hj1 = site_field(ref, s, i), site_field(ref, s, j)
+            hi2, hj2 = site_field(ref, x1, i), site_field(ref, x1, j)
+            S = abs(ai) ** 2 + abs(aj) ** 2
+            fwd = log_q_over_plain(net(wb, features(ai, aj, hi1, hj1, float(beta))), abs(ain) ** 2 / (abs(ain) ** 2 + abs(ajn) ** 2),
+                                   np.angle(ain) + np.angle(hi1), np.angle(ajn) + np.angle(hj1))
+            rev = log_q_over_plain(net(wb, features(ain, ajn, hi2, hj2, float(beta))), abs(ai) ** 2 / S,
+                                   np.angle(ai) + np.angle(hi2), np.angle(aj) + np.angle(hj2))
+            err = abs(float(r["log_q_ratio"]) - (rev - fwd))
+            worst = max(worst, err / (1.0 + 1e-3 * abs(rev - fwd)))
+            checked += 1
+        if r["accepted"]:
+            s[i], s[j] = ain, ajn
+    print("moves checked", checked, "worst", worst)
+    assert checked >= cap // 2
+    assert worst < 2e-3, worst
+
+
+def test_training_on_recorded_plain_moves_lowers_the_loss(ps):
+    N = 16
+    c = ps.default_config(N=N, nrep=32, seed=9, fmc_mode=0)
+    with ps.Engine(c) as eng:
+        eng.learn_init(seed=2, capacity=1 << 16, record_prob=1.0)
+        eng.set_proposal(ps.PROPOSAL_PLAIN_FIELDS)
+        T = np.geomspace(1.6, 0.2, 4)
+        eng.set_betas(np.repeat(1.0 / T, 8))
+        eng.sweep(200)
+        n, recs = eng.learn_records(1000)
+        assert n > 1000
+        assert np.all((recs[:, 8] > 0) & (recs[:, 8] < 1))
+        l0 = eng.learn_train(1, 2048, 0.0)
+        l1 = eng.learn_train(300, 2048, 3e-3)
+        print("loss", l0, "->", l1)
+        assert l1 < l0 - 0.2
+
+
+def test_proposal_state_errors(ps):
+    c = ps.default_config(N=8, nrep=4, seed=1)
+    with ps.Engine(c) as eng:
+        with pytest.raises(ps.PspinError):
+            eng.set_proposal(ps.PROPOSAL_LEARNED)          # no network yet
+        with pytest.raises(ps.PspinError):
+            eng.learn_train(1, 16, 1e-3)                   # no records yet
+        eng.learn_init(seed=1, capacity=8)
+        with pytest.raises(ps.PspinError):
+            eng.learn_train(1, 16, 1e-3)                   # ring still empty
+        with pytest.raises(ps.PspinError):
+            eng.set_proposal(7)
+    with ps.Engine(ps.default_config(N=8, nrep=4, seed=1), ps.PSPIN_SPARSE) as eng:
+        eng.learn_init(seed=1, capacity=8)
+        with pytest.raises(ps.PspinError):
+            eng.set_proposal(ps.PROPOSAL_PLAIN_FIELDS)     # dense only
