@@ -116,6 +116,8 @@ def load_library() -> ctypes.CDLL:
         "pspin_fmc_survivors_static": (ctypes.c_int, [ctypes.c_int, vp, ctypes.c_double, vp, vp]),
         "pspin_local_fields": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp, vp]),
         "pspin_set_proposal": (ctypes.c_int, [vp, ctypes.c_int]),
+        "pspin_observe_init": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+        "pspin_observe_get": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int]),
         "pspin_learn_init": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_float]),
         "pspin_learn_params": (ctypes.c_int, [vp, vp, vp]),
         "pspin_learn_train": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, vp]),
@@ -315,6 +317,21 @@ class Engine:
         prop = np.empty(NT - 1, np.int64)
         _check(self._lib.pspin_pt_get(self._h, sample, _ptr(perm), _ptr(acc), _ptr(prop)))
         return perm, acc, prop
+
+    def observe_init(self, temp_index: int, capacity: int) -> None:
+        _check(self._lib.pspin_observe_init(self._h, int(temp_index), int(capacity)))
+
+    def observe_get(self):
+        """(E [rows, samples, nrep], q [rows, samples, nrep(nrep-1)/2]) at the observed slot."""
+        nr = self.nrep_per_temp
+        npairs = nr * (nr - 1) // 2
+        n = ctypes.c_int64(0)
+        _check(self._lib.pspin_observe_get(self._h, ctypes.byref(n), None, None, 0))
+        rows = n.value
+        E = np.empty((max(rows, 1), self.n_samples, nr), np.float64)
+        q = np.empty((max(rows, 1), self.n_samples, max(npairs, 1)), np.float64)
+        _check(self._lib.pspin_observe_get(self._h, ctypes.byref(n), _ptr(E), _ptr(q), rows))
+        return E[:rows], q[:rows, :, :npairs]
 
     # -- all-site local fields ------------------------------------------------------
     def local_fields(self, sample: int = 0, method: int = 0):

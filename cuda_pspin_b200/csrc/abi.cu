@@ -154,6 +154,8 @@ struct pspin_state {
     int2* d_entries = nullptr;
     int64_t* d_chunk_start = nullptr;
     int* d_site_chunks = nullptr;
+    int* d_pair_chunks = nullptr;       // pair sub-lists, built on the first two-pass proposal
+    int64_t ent_total = 0, chunk_total = 0;
     Q64* d_q64 = nullptr;
     double* d_g2 = nullptr;
     double* d_g4re = nullptr;
@@ -193,6 +195,11 @@ struct pspin_state {
     int adam_t = 0;
     uint64_t learn_seed = 0;
 
+    // observable series at one temperature slot
+    double *d_obs_E = nullptr, *d_obs_q = nullptr;
+    int obs_t = -1, obs_cap = 0;
+    long long obs_sweep0 = 0;
+
     // trace
     pspin_move_record* d_trace = nullptr;
     long long trace_sweep0 = 0;
@@ -215,7 +222,7 @@ static void free_state(pspin_state* s) {
                     s->d_beta_sched, s->d_perm, s->d_drand, s->d_ex_acc, s->d_ex_prop, s->d_trace,
                     s->d_tc_w, s->d_tc_x, s->d_tc_f, s->d_tc_ws, s->d_tc_h, s->d_f64_h, s->d_tc_e,
                     s->d_w32, s->d_adam_m, s->d_adam_v, s->d_grad, s->d_wbf, s->d_records, s->d_rec_count,
-                    s->d_save, s->d_loss, s->d_idx};
+                    s->d_save, s->d_loss, s->d_idx, s->d_obs_E, s->d_obs_q, s->d_pair_chunks};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& e : s->ev_pool) {
@@ -860,6 +867,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         d.q_off = q_total;
         d.nq = (int64_t)q64[k].size();
         d.g2_off = g2_total;
+        d.pair_off = -1;
         uint64_t pk = h.cfg.seed + 7000;
         const uint64_t key = splitmix64(pk);
         d.pair_key0 = (uint32_t)key;
@@ -901,6 +909,8 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         }
         chunk_start[chunk_total] = eoff;
     }
+    s->ent_total = ent_total;
+    s->chunk_total = chunk_total;
     // units: replica blocks of 32, heaviest samples first
     for (int k = 0; k < n; k++)
         for (int rb = 0; rb < s->hs[k].R; rb += kRepBlock)
@@ -999,6 +1009,7 @@ static int launch_chunk(pspin_state* s, int nsweeps, bool exchange) {
     p.entries = s->d_entries;
     p.chunk_start = s->d_chunk_start;
     p.site_chunks = s->d_site_chunks;
+    p.pair_chunks = s->d_pair_chunks;
     p.sweep_counter = s->d_sweep_counter;
     p.nsweeps = nsweeps;
     p.warps = s->warps;
@@ -1053,6 +1064,25 @@ static int launch_chunk(pspin_state* s, int nsweeps, bool exchange) {
     x.do_exchange = exchange ? 1 : 0;
     CK(launch_exchange(x, s->st));
     s->kernel_launches++;
+    if (exchange && s->obs_cap > 0) {
+        ObserveParams o{};
+        o.n_samples = s->S;
+        o.NT = s->pt_NT;
+        o.nrep = s->pt_nrep;
+        o.temp_index = s->obs_t;
+        o.capacity = s->obs_cap;
+        o.pt_freq = s->pt_freq;
+        o.samples = s->d_samples;
+        o.spins = s->d_spins;
+        o.energy = s->d_E;
+        o.perm = s->d_perm;
+        o.sweep_counter = s->d_sweep_counter;
+        o.sweep0 = s->obs_sweep0;
+        o.E_out = s->d_obs_E;
+        o.q_out = s->d_obs_q;
+        CK(launch_observe(o, s->st));
+        s->kernel_launches++;
+    }
     s->sweeps_done += nsweeps;
     s->since_resync += nsweeps;
     if (s->opt.resync_every > 0 && s->since_resync >= s->opt.resync_every) {
@@ -1280,6 +1310,49 @@ extern "C" int pspin_pt_get(pspin_state* s, int sample, int32_t* perm, int64_t* 
     return PSPIN_OK;
 }
 
+extern "C" int pspin_observe_init(pspin_state* s, int temp_index, int capacity) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (s->pt_NT < 2) return fail(PSPIN_ERR_STATE, "pspin_pt_init has not been called");
+    if (temp_index < 0 || temp_index >= s->pt_NT || capacity < 0)
+        return fail(PSPIN_ERR_ARG, "temperature index %d outside [0, %d) or negative capacity", temp_index, s->pt_NT);
+    cudaFree(s->d_obs_E);
+    cudaFree(s->d_obs_q);
+    s->d_obs_E = nullptr;
+    s->d_obs_q = nullptr;
+    s->obs_cap = 0;
+    if (capacity == 0) return PSPIN_OK;
+    const int nr = s->pt_nrep, npairs = nr * (nr - 1) / 2;
+    int rc;
+    if ((rc = dalloc(&s->d_obs_E, (size_t)capacity * s->S * nr)) ||
+        (rc = dalloc(&s->d_obs_q, (size_t)capacity * s->S * std::max(npairs, 1))))
+        return rc;
+    CK(cudaMemcpyAsync(&s->obs_sweep0, s->d_sweep_counter, sizeof(long long), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    s->obs_t = temp_index;
+    s->obs_cap = capacity;
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_observe_get(pspin_state* s, int64_t* n_rows, double* energy, double* overlap, int max_rows) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (s->obs_cap <= 0) return fail(PSPIN_ERR_STATE, "pspin_observe_init has not been called");
+    long long counter = 0;
+    CK(cudaMemcpyAsync(&counter, s->d_sweep_counter, sizeof(long long), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    long long n = (counter - s->obs_sweep0) / s->pt_freq;
+    n = std::max(0LL, std::min<long long>(n, s->obs_cap));
+    if (n_rows) *n_rows = n;
+    const long long m = std::min<long long>(n, std::max(max_rows, 0));
+    const int nr = s->pt_nrep, npairs = nr * (nr - 1) / 2;
+    if (energy && m > 0)
+        CK(cudaMemcpyAsync(energy, s->d_obs_E, (size_t)m * s->S * nr * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    if (overlap && m > 0 && npairs > 0)
+        CK(cudaMemcpyAsync(overlap, s->d_obs_q, (size_t)m * s->S * npairs * sizeof(double), cudaMemcpyDeviceToHost,
+                           s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
 extern "C" int pspin_pt_sweeps_done(pspin_state* s, int64_t* sweeps) {
     if (!s || !sweeps) return fail(PSPIN_ERR_ARG, "null argument");
     *sweeps = s->sweeps_done;
@@ -1395,6 +1468,93 @@ extern "C" int pspin_local_fields(pspin_state* s, int sample, int method, double
 }
 
 // ------------------------------------------------------------------ learned proposal
+// Pair sub-lists for the two-pass sweep: rebuilt from the FP64 quartet table
+// (same couplings, rounded to FP32 like the site lists) and appended to the
+// entry and chunk arrays; d_pair_chunks indexes them per sample.
+static int ensure_pair_lists(pspin_state* s) {
+    if (s->d_pair_chunks) return PSPIN_OK;
+    const int n = s->S;
+    std::vector<std::vector<Q64>> q(n);
+    for (int k = 0; k < n; k++) {
+        q[k].resize((size_t)s->sd[k].nq);
+        if (s->sd[k].nq)
+            CK(cudaMemcpyAsync(q[k].data(), s->d_q64 + s->sd[k].q_off, q[k].size() * sizeof(Q64),
+                               cudaMemcpyDeviceToHost, s->st));
+    }
+    CK(cudaStreamSynchronize(s->st));
+    std::vector<SiteLists> pl(n);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < n; k++) {
+        std::vector<QuartetRec> recs(q[k].size());
+        for (size_t t = 0; t < q[k].size(); t++) {
+            const Q64& e = q[k][t];
+            recs[t] = QuartetRec{e.i, e.j, e.k, e.lch & 0x3fff, e.lch >> 14, e.g};
+        }
+        std::vector<Q64>().swap(q[k]);
+        build_pair_lists(s->hs[k].N, s->hs[k].g2re.data(), s->hs[k].h2_active, recs, pl[k]);
+    }
+    int64_t ent_new = 0, chunk_new = 0, idx_total = 0;
+    for (int k = 0; k < n; k++) {
+        ent_new += (int64_t)pl[k].entries.size();
+        chunk_new += (int64_t)pl[k].chunk_start.size();
+        idx_total += (int64_t)pl[k].site_chunks.size();
+    }
+    if (s->chunk_total + chunk_new >= (1ll << 31)) return fail(PSPIN_ERR_ARG, "too many list chunks for the pair sub-lists");
+    std::vector<int2> ent((size_t)ent_new);
+    std::vector<int64_t> cs((size_t)chunk_new + 1);
+    std::vector<int> pc((size_t)idx_total);
+    std::vector<int64_t> pair_off(n);
+    int64_t eoff = 0, coff = 0, ioff = 0;
+    for (int k = 0; k < n; k++) {
+        std::copy(pl[k].entries.begin(), pl[k].entries.end(), ent.begin() + eoff);
+        for (size_t t = 0; t < pl[k].chunk_start.size(); t++) cs[coff + t] = pl[k].chunk_start[t] + eoff + s->ent_total;
+        for (size_t t = 0; t < pl[k].site_chunks.size(); t++)
+            pc[ioff + t] = (int)(pl[k].site_chunks[t] + coff + s->chunk_total);
+        pair_off[k] = ioff;
+        eoff += (int64_t)pl[k].entries.size();
+        coff += (int64_t)pl[k].chunk_start.size();
+        ioff += (int64_t)pl[k].site_chunks.size();
+        pl[k] = SiteLists();
+    }
+    cs[chunk_new] = s->ent_total + ent_new;
+    int2* d_ent = nullptr;
+    int64_t* d_cs = nullptr;
+    int* d_pc = nullptr;
+    int rc;
+    if ((rc = dalloc(&d_ent, (size_t)(s->ent_total + ent_new))) ||
+        (rc = dalloc(&d_cs, (size_t)(s->chunk_total + chunk_new + 1))) || (rc = dalloc(&d_pc, (size_t)idx_total))) {
+        cudaFree(d_ent); cudaFree(d_cs); cudaFree(d_pc);
+        return rc;
+    }
+    std::vector<SampleDev> sd = s->sd;
+    for (int k = 0; k < n; k++) sd[k].pair_off = pair_off[k];
+    cudaError_t e = cudaMemcpyAsync(d_ent, s->d_entries, s->ent_total * sizeof(int2), cudaMemcpyDeviceToDevice, s->st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_ent + s->ent_total, ent.data(), ent.size() * sizeof(int2), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_cs, s->d_chunk_start, s->chunk_total * sizeof(int64_t), cudaMemcpyDeviceToDevice, s->st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_cs + s->chunk_total, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_pc, pc.data(), pc.size() * sizeof(int), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->d_samples, sd.data(), sd.size() * sizeof(SampleDev), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) {
+        cudaFree(d_ent); cudaFree(d_cs); cudaFree(d_pc);
+        return fail(PSPIN_ERR_CUDA, "pair sub-list upload: %s", cudaGetErrorString(e));
+    }
+    s->sd = sd;
+    cudaFree(s->d_entries);
+    cudaFree(s->d_chunk_start);
+    s->d_entries = d_ent;
+    s->d_chunk_start = d_cs;
+    s->d_pair_chunks = d_pc;
+    s->ent_total += ent_new;
+    s->chunk_total += chunk_new;
+    return PSPIN_OK;
+}
+
 extern "C" int pspin_set_proposal(pspin_state* s, int proposal) {
     if (!s) return fail(PSPIN_ERR_ARG, "null handle");
     if (proposal < PSPIN_PROPOSAL_PLAIN || proposal > PSPIN_PROPOSAL_LEARNED)
@@ -1403,6 +1563,7 @@ extern "C" int pspin_set_proposal(pspin_state* s, int proposal) {
         return fail(PSPIN_ERR_UNSUPPORTED, "the learned proposal is built for the dense (spherical) variant");
     if (proposal == PSPIN_PROPOSAL_LEARNED && !s->d_wbf)
         return fail(PSPIN_ERR_STATE, "pspin_learn_init has not been called");
+    if (proposal != PSPIN_PROPOSAL_PLAIN) TRY(ensure_pair_lists(s));
     s->proposal = proposal;
     return PSPIN_OK;
 }

@@ -65,6 +65,7 @@ struct SampleDev {
     int64_t q_off;         // index into the Q64 table
     int64_t nq;            // active (quartet, channel) pairs in the Q64 table
     int64_t g2_off;        // index into g2 (N*N doubles)
+    int64_t pair_off;      // index into the pair sub-list chunks (N(N-1)*33 entries), -1: not built
     uint32_t pair_key0, pair_key1;
 };
 
@@ -92,6 +93,7 @@ struct SweepParams {
     const int2* entries;
     const int64_t* chunk_start;
     const int* site_chunks;
+    const int* pair_chunks;           // pair sub-lists (two-pass proposals), or null
     const long long* sweep_counter;   // global sweep index at launch start
     int nsweeps;
     int warps;                        // warps per unit (divides 32)
@@ -142,5 +144,21 @@ struct ExchangeParams {
     int do_exchange;
 };
 cudaError_t launch_exchange(const ExchangeParams& p, cudaStream_t st);
+
+// Observable series at one temperature slot, written after each exchange
+// step at row (sweep_counter - sweep0) / pt_freq - 1 (device counter, so a
+// captured launch records into the right row).
+struct ObserveParams {
+    int n_samples, NT, nrep, temp_index, capacity, pt_freq;
+    const SampleDev* samples;
+    const float2* spins;
+    const double* energy;
+    const int* perm;
+    const long long* sweep_counter;
+    long long sweep0;
+    double* E_out;            // [capacity][S][nrep]
+    double* q_out;            // [capacity][S][nrep*(nrep-1)/2]
+};
+cudaError_t launch_observe(const ObserveParams& p, cudaStream_t st);
 
 }  // namespace pspin

@@ -73,6 +73,69 @@ static void pack_site(const std::vector<int2>& site, const std::vector<std::pair
     sc[kSplit] = (int)out.chunk_start.size();
 }
 
+// Sorts one list's records by (p, o1, o2), cuts groups of equal (p, o1) at
+// kGroupMax data entries and packs them as list `id`.
+static void group_and_pack(std::vector<Rec>& v, int id, std::vector<int2>& site,
+                           std::vector<std::pair<int64_t, int64_t>>& groups, SiteLists& out) {
+    std::sort(v.begin(), v.end(), [](const Rec& a, const Rec& b) {
+        return a.key != b.key ? a.key < b.key : a.o2 < b.o2;
+    });
+    site.clear();
+    groups.clear();
+    size_t t = 0;
+    while (t < v.size()) {
+        size_t e = t;
+        while (e < v.size() && v[e].key == v[t].key && (int)(e - t) < kGroupMax) e++;
+        const int64_t gb = (int64_t)site.size();
+        site.push_back(make_int2((int)(e - t), v[t].key));
+        for (size_t u = t; u < e; u++) {
+            int bits;
+            std::memcpy(&bits, &v[u].g, sizeof(int));
+            site.push_back(make_int2(bits, v[u].o2));
+        }
+        groups.push_back({gb, (int64_t)site.size()});
+        t = e;
+    }
+    pack_site(site, groups, id, out);
+}
+
+void build_pair_lists(int N, const double* g2re, int h2_active, const std::vector<QuartetRec>& qs,
+                      SiteLists& out) {
+    const int npairs = N * (N - 1) / 2;
+    auto list_id = [](int m, int x) {   // m's terms that contain x
+        return m < x ? 2 * (x * (x - 1) / 2 + m) : 2 * (m * (m - 1) / 2 + x) + 1;
+    };
+    std::vector<std::vector<Rec>> per((size_t)2 * npairs);
+    for (const QuartetRec& r : qs) {
+        const int q[4] = {r.i, r.j, r.k, r.l};
+        const float g = (float)r.g;
+        for (int pos = 0; pos < 4; pos++) {
+            int p, o1, o2;
+            class_of(q, r.ch, pos, p, o1, o2);
+            const Rec rec{(p << 16) | o1, o2, g};
+            per[list_id(q[pos], p)].push_back(rec);
+            per[list_id(q[pos], o1)].push_back(rec);
+            per[list_id(q[pos], o2)].push_back(rec);
+        }
+    }
+    if (h2_active)
+        for (int m = 0; m < N; m++)
+            for (int j = 0; j < N; j++) {
+                if (j == m) continue;
+                const double g = g2re[(size_t)m * N + j];
+                if (g != 0.0) per[list_id(m, j)].push_back(Rec{(N << 16) | N, j, (float)g});
+            }
+    out.entries.clear();
+    out.chunk_start.clear();
+    out.site_chunks.assign((size_t)2 * npairs * (kSplit + 1), 0);
+    std::vector<std::pair<int64_t, int64_t>> groups;
+    std::vector<int2> site;
+    for (int id = 0; id < 2 * npairs; id++) {
+        group_and_pack(per[id], id, site, groups, out);
+        std::vector<Rec>().swap(per[id]);
+    }
+}
+
 void build_site_lists(int N, const double* g2re, int h2_active, const std::vector<QuartetRec>& qs,
                       SiteLists& out) {
     std::vector<std::vector<Rec>> per(N);
@@ -103,30 +166,7 @@ void build_site_lists(int N, const double* g2re, int h2_active, const std::vecto
     out.site_chunks.assign((size_t)N * (kSplit + 1), 0);
     std::vector<std::pair<int64_t, int64_t>> groups;   // [begin, end) in a site-local list
     std::vector<int2> site;
-    for (int m = 0; m < N; m++) {
-        std::vector<Rec>& v = per[m];
-        std::sort(v.begin(), v.end(), [](const Rec& a, const Rec& b) {
-            return a.key != b.key ? a.key < b.key : a.o2 < b.o2;
-        });
-        // groups of equal (p, o1), cut at kGroupMax data entries
-        site.clear();
-        groups.clear();
-        size_t t = 0;
-        while (t < v.size()) {
-            size_t e = t;
-            while (e < v.size() && v[e].key == v[t].key && (int)(e - t) < kGroupMax) e++;
-            const int64_t gb = (int64_t)site.size();
-            site.push_back(make_int2((int)(e - t), v[t].key));
-            for (size_t u = t; u < e; u++) {
-                int bits;
-                std::memcpy(&bits, &v[u].g, sizeof(int));
-                site.push_back(make_int2(bits, v[u].o2));
-            }
-            groups.push_back({gb, (int64_t)site.size()});
-            t = e;
-        }
-        pack_site(site, groups, m, out);
-    }
+    for (int m = 0; m < N; m++) group_and_pack(per[m], m, site, groups, out);
 }
 
 static inline int64_t encode_sorted(int a, int b, int c, int d) {

@@ -20,6 +20,12 @@ struct SiteLists {
 
 void build_site_lists(int N, const double* g2re, int h2_active, const std::vector<QuartetRec>& qs,
                       SiteLists& out);
+// Sub-lists of the terms that couple the two sites of a pair (same group
+// format): for i < j and P = j(j-1)/2 + i, list 2P holds site i's terms that
+// contain a_j, list 2P+1 site j's terms that contain a_i.  Each term of a
+// site list is in 3 of them (one per other site of its quartet).
+void build_pair_lists(int N, const double* g2re, int h2_active, const std::vector<QuartetRec>& qs,
+                      SiteLists& out);
 // fully connected tiles from the dense g4 (channel 0 everywhere) and g2
 void build_site_tiles_fc(int N, const double* g2re, int h2_active, const double* g4re, SiteLists& out);
 void build_q64(const std::vector<QuartetRec>& qs, std::vector<Q64>& out);

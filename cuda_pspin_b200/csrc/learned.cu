@@ -4,8 +4,10 @@
 // the network's training kernels (forward, backward, Adam).
 //
 // Two field passes per move.  Pass 1 reads site i's and site j's lists at
-// the current state x: h_i(x), h_j(x) (the proposal's features).  The
-// proposal is then written into both slots and pass 2 gives h_i(x'), h_j(x')
+// the current state x: h_i(x), h_j(x) (the proposal's features).  Pass 2
+// reads only the pair's sub-lists (the terms of h_i that contain a_j and of
+// h_j that contain a_i, about 3/N of a site list) with the changes da_i,
+// da_j in the pair's slots, giving h_i(x') - h_i(x) and h_j(x') - h_j(x)
 // (the reverse density's features).  E is affine in each site, so
 //     dE = -Re[da_i h_i(x')] - Re[da_j h_j(x)]
 // exactly (h_i(x') is h_i with a_j' in place, h_j(x) is h_j with a_i).
@@ -26,37 +28,54 @@ struct LearnParams {
     float rec_prob;
 };
 
-// Inference for the 32 replicas of warp 0: activations in shared memory
-// [64][32] (lane-contiguous), weights in shared memory (BF16, broadcast reads).
-__device__ __forceinline__ void mlp_warp(const __nv_bfloat16* __restrict__ w, const float* f, float* act1,
-                                         float* act2, int lane, float* out) {
-    for (int o = 0; o < kMlpHidden; o++) {
-        float z = __bfloat162float(w[kOffB1 + o]);
+// Network evaluation for the CTA's 32 replicas by all its warps: features
+// feat[8][32] -> act1[64][32] -> act2[64][32] -> outs[26][32], shared memory,
+// lane-contiguous; BF16 weights in shared memory (broadcast reads), FP32
+// accumulation.  Warp w computes units w, w+W, ...; a barrier after each
+// layer (called by every thread of the CTA).
+__device__ __forceinline__ void mlp_block(const __nv_bfloat16* __restrict__ w, const float* feat, float* act1,
+                                          float* act2, float* outs, int warp, int W, int lane) {
+    for (int u = warp; u < kMlpHidden; u += W) {
+        float z = __bfloat162float(w[kOffB1 + u]);
 #pragma unroll
-        for (int i = 0; i < kMlpIn; i++) z = fmaf(__bfloat162float(w[kOffW1 + o * kMlpIn + i]), f[i], z);
-        act1[o * 32 + lane] = tanhf(z);
+        for (int i = 0; i < kMlpIn; i++) z = fmaf(__bfloat162float(w[kOffW1 + u * kMlpIn + i]), feat[i * 32 + lane], z);
+        act1[u * 32 + lane] = tanhf(z);
     }
-    for (int o = 0; o < kMlpHidden; o++) {
-        float z = __bfloat162float(w[kOffB2 + o]);
+    __syncthreads();
+    for (int u = warp; u < kMlpHidden; u += W) {
+        float z = __bfloat162float(w[kOffB2 + u]);
+        const __nv_bfloat162* row = reinterpret_cast<const __nv_bfloat162*>(w + kOffW2 + u * kMlpHidden);
 #pragma unroll 8
-        for (int i = 0; i < kMlpHidden; i++)
-            z = fmaf(__bfloat162float(w[kOffW2 + o * kMlpHidden + i]), act1[i * 32 + lane], z);
-        act2[o * 32 + lane] = tanhf(z);
+        for (int i = 0; i < kMlpHidden / 2; i++) {
+            const float2 wv = __bfloat1622float2(row[i]);
+            z = fmaf(wv.x, act1[(2 * i) * 32 + lane], z);
+            z = fmaf(wv.y, act1[(2 * i + 1) * 32 + lane], z);
+        }
+        act2[u * 32 + lane] = tanhf(z);
     }
-    for (int o = 0; o < kMlpOut; o++) {
-        float z = __bfloat162float(w[kOffB3 + o]);
+    __syncthreads();
+    for (int u = warp; u < kMlpOut; u += W) {
+        float z = __bfloat162float(w[kOffB3 + u]);
+        const __nv_bfloat162* row = reinterpret_cast<const __nv_bfloat162*>(w + kOffW3 + u * kMlpHidden);
 #pragma unroll 8
-        for (int i = 0; i < kMlpHidden; i++)
-            z = fmaf(__bfloat162float(w[kOffW3 + o * kMlpHidden + i]), act2[i * 32 + lane], z);
-        out[o] = z;
+        for (int i = 0; i < kMlpHidden / 2; i++) {
+            const float2 wv = __bfloat1622float2(row[i]);
+            z = fmaf(wv.x, act2[(2 * i) * 32 + lane], z);
+            z = fmaf(wv.y, act2[(2 * i + 1) * 32 + lane], z);
+        }
+        outs[u * 32 + lane] = z;
     }
+    __syncthreads();
 }
 
 __device__ __forceinline__ float argf(float2 a) { return atan2f(a.y, a.x); }
 
+// feat[8][32] + act1, act2 [64][32] + outs[26][32] floats, then the BF16 weights
+constexpr int kMlpSmemFloats = (kMlpIn + 2 * kMlpHidden + kMlpOut) * 32;
+
 inline size_t learned_smem_bytes(int N, int warps) {
-    return sweep_smem_bytes(N, warps) + (size_t)kMlpParams * sizeof(__nv_bfloat16) + 16 +
-           (size_t)2 * kMlpHidden * 32 * sizeof(float);
+    return sweep_smem_bytes(N, warps) + (size_t)kMlpSmemFloats * sizeof(float) +
+           (size_t)kMlpParams * sizeof(__nv_bfloat16) + 16;
 }
 
 __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams P, const LearnParams L) {
@@ -65,15 +84,18 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
     const SampleDev S = P.samples[U.sample];
     const int N = S.N, R = S.R;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = P.warps;
+    const bool learned = L.mode == 2;
     float2* sp = reinterpret_cast<float2*>(smem_raw);
     float4* red = reinterpret_cast<float4*>(sp + (size_t)(N + 1) * kRepBlock);
     int2* ring_all = reinterpret_cast<int2*>(red + (size_t)W * kRepBlock);
     int2* ring = ring_all + (size_t)warp * kStages * kStage;
     uint64_t* bars_all = reinterpret_cast<uint64_t*>(ring_all + (size_t)W * kStages * kStage);
     uint64_t* bars = bars_all + warp * kStages;
-    float* act1 = reinterpret_cast<float*>(bars_all + W * kStages);
+    float* feat = reinterpret_cast<float*>(bars_all + W * kStages);
+    float* act1 = feat + kMlpIn * 32;
     float* act2 = act1 + kMlpHidden * 32;
-    __nv_bfloat16* wsm = reinterpret_cast<__nv_bfloat16*>(act2 + kMlpHidden * 32);
+    float* outs = act2 + kMlpHidden * 32;
+    __nv_bfloat16* wsm = reinterpret_cast<__nv_bfloat16*>(outs + kMlpOut * 32);
 
     const bool active = lane < U.rep_count;
     const int64_t gr = S.rep_off + U.rep_begin + lane;
@@ -84,7 +106,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
         sp[idx] = v;
     }
     if (threadIdx.x < kRepBlock) sp[N * kRepBlock + threadIdx.x] = make_float2(1.f, 0.f);
-    if (L.mode == 2)
+    if (learned)
         for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) wsm[i] = L.w[i];
 
     double E = 0.0, beta_d = 0.0;
@@ -101,17 +123,17 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
     }
     const long long sweep0 = *P.sweep_counter;
     const int steps = N / 2, total = P.nsweeps * steps;
-    Stream st;
+    Stream<4> st;
     st.key0 = S.pair_key0;
     st.key1 = S.pair_key1;
     st.N = N;
     st.site_chunks = P.site_chunks + S.split_off;
+    st.pair_chunks = P.pair_chunks + S.pair_off;
     st.sweep0 = sweep0;
     st.steps = steps;
     st.total = total;
     st.part0 = warp * (kSplit / W);
     st.part1 = (warp + 1) * (kSplit / W);
-    st.lists = 4;
     if (lane == 0) {
         for (int s = 0; s < kStages; s++) mbar_init(bars + s, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -136,7 +158,8 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
     for (int s = 0; s < kStages; s++) issue();
     __syncthreads();
 
-    // one field pass over this warp's share of site i0's and site j0's lists
+    // one pass over this warp's share of two lists: the sites' lists (base 0)
+    // or the pair's sub-lists (base 2, always in the group format)
     auto pass = [&](int m, int base, float* h) {
         for (int which = base; which < base + 2; which++) {
             int c, c_end;
@@ -146,7 +169,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
                 if (ok_wait) ok_wait = mbar_wait(bars + slot, (consumed / kStages) & 1u, P.status);
                 const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
                 const int k2 = 2 * (which & 1);
-                if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
+                if (S.fc_tiles && which < 2) accumulate_tiles(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
                 else accumulate_chunk(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
                 consumed++;
                 __syncwarp();
@@ -155,6 +178,18 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
             }
         }
     };
+    // partial sums of all warps -> warp 0 (one barrier)
+    auto reduce = [&](const float* h) {
+        red[warp * kRepBlock + lane] = make_float4(h[0], h[1], h[2], h[3]);
+        __syncthreads();
+        float4 hs = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (warp == 0)
+            for (int w = 0; w < W; w++) {
+                const float4 v = red[w * kRepBlock + lane];
+                hs.x += v.x; hs.y += v.y; hs.z += v.z; hs.w += v.w;
+            }
+        return hs;
+    };
 
     for (int m = 0; m < total; m++) {
         const long long sw = sweep0 + m / steps;
@@ -162,29 +197,33 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
         int i0, j0;
         pair_pick(S.pair_key0, S.pair_key1, (uint64_t)sw, (uint32_t)k, N, i0, j0);
 
+        // ---- fields at x: h_i (with a_j), h_j (with a_i) ---------------------------
         float h[4] = {0.f, 0.f, 0.f, 0.f};
         pass(m, 0, h);
-        red[warp * kRepBlock + lane] = make_float4(h[0], h[1], h[2], h[3]);
-        __syncthreads();
-
-        // ---- proposal (warp 0) -------------------------------------------------
-        float2 ai = make_float2(0.f, 0.f), aj = ai, ain = ai, ajn = ai, hi1 = ai, hj1 = ai;
-        float cu = 0.f, lq_fwd = 0.f, lq_ratio = 0.f, tn = 0.5f, psi_i = 0.f, psi_j = 0.f;
+        const float4 hs1 = reduce(h);
+        float2 ai = make_float2(0.f, 0.f), aj = ai, ain = ai, ajn = ai;
+        const float2 hi1 = make_float2(hs1.x, hs1.y), hj1 = make_float2(hs1.z, hs1.w);
+        float cu = 0.f, lq_fwd = 0.f, lq_ratio = 0.f, tn = 0.5f, psi_i = 0.f, psi_j = 0.f, Ssum = 1.f;
         bool ok = true;
-        MoveStream g;
+        MoveStream g{k0, k1, (uint32_t)k, (uint32_t)sw, (uint32_t)((uint64_t)sw >> 32), 0u, 4u, U4{0, 0, 0, 0}};
         if (warp == 0) {
-            float4 hs = red[lane];
-            for (int w = 1; w < W; w++) {
-                const float4 v = red[w * kRepBlock + lane];
-                hs.x += v.x; hs.y += v.y; hs.z += v.z; hs.w += v.w;
-            }
-            hi1 = make_float2(hs.x, hs.y);
-            hj1 = make_float2(hs.z, hs.w);
             ai = sp[i0 * kRepBlock + lane];
             aj = sp[j0 * kRepBlock + lane];
-            const float Ssum = fmaf(ai.x, ai.x, ai.y * ai.y) + fmaf(aj.x, aj.x, aj.y * aj.y);
-            g = MoveStream{k0, k1, (uint32_t)k, (uint32_t)sw, (uint32_t)((uint64_t)sw >> 32), 0u, 4u, U4{0, 0, 0, 0}};
-            if (L.mode == 1) {
+            Ssum = fmaf(ai.x, ai.x, ai.y * ai.y) + fmaf(aj.x, aj.x, aj.y * aj.y);
+            if (learned) {
+                float f[kMlpIn];
+                pair_features(ai, aj, hi1, hj1, beta, f);
+#pragma unroll
+                for (int i = 0; i < kMlpIn; i++) feat[i * 32 + lane] = f[i];
+            }
+        }
+        // ---- proposal -------------------------------------------------------------
+        if (learned) {
+            __syncthreads();
+            mlp_block(wsm, feat, act1, act2, outs, warp, W, lane);
+        }
+        if (warp == 0) {
+            if (!learned) {
                 const U4 w = move_words(k0, k1, (uint64_t)sw, (uint32_t)k);
                 propose<0>(ai, aj, w, ain, ajn);
                 cu = u01f(w.w);
@@ -192,9 +231,9 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
                 psi_i = argf(ain) + argf(hi1);
                 psi_j = argf(ajn) + argf(hj1);
             } else {
-                float f[kMlpIn], out[kMlpOut];
-                pair_features(ai, aj, hi1, hj1, beta, f);
-                mlp_warp(wsm, f, act1, act2, lane, out);
+                float out[kMlpOut];
+#pragma unroll
+                for (int o = 0; o < kMlpOut; o++) out[o] = outs[o * 32 + lane];
                 ProposalParams pp;
                 decode_outputs(out, pp);
                 ok = sample_move(g, pp, tn, psi_i, psi_j);
@@ -212,52 +251,61 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
                 }
                 cu = g.uniform();
             }
-            sp[i0 * kRepBlock + lane] = ain;
-            sp[j0 * kRepBlock + lane] = ajn;
+            // the pair's slots hold the changes while the sub-lists are read:
+            // every term there contains exactly one of a_i, a_j (linearly or
+            // conjugated), so the sums are h_i(x') - h_i(x) and h_j(x') - h_j(x)
+            sp[i0 * kRepBlock + lane] = make_float2(ain.x - ai.x, ain.y - ai.y);
+            sp[j0 * kRepBlock + lane] = make_float2(ajn.x - aj.x, ajn.y - aj.y);
         }
         __syncthreads();
 
-        // ---- fields at the proposed state ---------------------------------------
+        // ---- field changes from the pair's sub-lists --------------------------------
         h[0] = h[1] = h[2] = h[3] = 0.f;
         pass(m, 2, h);
-        red[warp * kRepBlock + lane] = make_float4(h[0], h[1], h[2], h[3]);
-        __syncthreads();
-
+        const float4 dh = reduce(h);
+        float dE = 0.f;
+        float2 hi2 = hi1, hj2 = hj1;
         if (warp == 0) {
-            float4 hs = red[lane];
-            for (int w = 1; w < W; w++) {
-                const float4 v = red[w * kRepBlock + lane];
-                hs.x += v.x; hs.y += v.y; hs.z += v.z; hs.w += v.w;
-            }
-            const float2 hi2 = make_float2(hs.x, hs.y), hj2 = make_float2(hs.z, hs.w);
+            hi2 = make_float2(hi1.x + dh.x, hi1.y + dh.y);
+            hj2 = make_float2(hj1.x + dh.z, hj1.y + dh.w);
             const float dix = ain.x - ai.x, diy = ain.y - ai.y, djx = ajn.x - aj.x, djy = ajn.y - aj.y;
-            const float dE = -fmaf(dix, hi2.x, -diy * hi2.y) - fmaf(djx, hj1.x, -djy * hj1.y);
+            dE = -fmaf(dix, hi2.x, -diy * hi2.y) - fmaf(djx, hj1.x, -djy * hj1.y);
+            if (learned) {
+                float f[kMlpIn];
+                pair_features(ain, ajn, hi2, hj2, beta, f);
+#pragma unroll
+                for (int i = 0; i < kMlpIn; i++) feat[i * 32 + lane] = f[i];
+            }
+        }
+        if (learned) {
+            __syncthreads();
+            mlp_block(wsm, feat, act1, act2, outs, warp, W, lane);
+        }
+        if (warp == 0) {
             bool accept;
-            if (L.mode == 1) {
+            if (!learned) {
                 if (beta_d == 0.0) accept = true;
                 else accept = (dE <= 0.f) || (cu < expf(-beta * dE));
             } else {
-                float f[kMlpIn], out[kMlpOut];
-                pair_features(ain, ajn, hi2, hj2, beta, f);
-                mlp_warp(wsm, f, act1, act2, lane, out);
+                float out[kMlpOut];
+#pragma unroll
+                for (int o = 0; o < kMlpOut; o++) out[o] = outs[o * 32 + lane];
                 ProposalParams pr;
                 decode_outputs(out, pr);
-                const float Ssum = fmaf(ai.x, ai.x, ai.y * ai.y) + fmaf(aj.x, aj.x, aj.y * aj.y);
                 const float t = fmaf(ai.x, ai.x, ai.y * ai.y) / Ssum;
                 const float lq_rev = log_learned_density(pr, t, argf(ai) + argf(hi2), argf(aj) + argf(hj2)) -
                                      log_plain_density(t);
                 lq_ratio = lq_rev - lq_fwd;
                 accept = ok && (logf(cu) < -beta * dE + lq_ratio);
             }
+            sp[i0 * kRepBlock + lane] = accept ? ain : ai;
+            sp[j0 * kRepBlock + lane] = accept ? ajn : aj;
             if (accept) {
                 E += (double)dE;
                 nacc++;
-            } else {
-                sp[i0 * kRepBlock + lane] = ai;
-                sp[j0 * kRepBlock + lane] = aj;
             }
             nprop++;
-            if (L.mode == 1 && accept && active && L.records != nullptr && u01f(g.next()) < L.rec_prob) {
+            if (!learned && accept && active && L.records != nullptr && u01f(g.next()) < L.rec_prob) {
                 float f[kMlpIn];
                 pair_features(ai, aj, hi1, hj1, beta, f);
                 const unsigned long long slot = atomicAdd(L.rec_count, 1ull) % (unsigned long long)L.rec_cap;
@@ -300,6 +348,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
 cudaError_t launch_learned_sweep(const SweepParams& p, const LearnParams& l, int n_units, int max_N,
                                  cudaStream_t st) {
     if (n_units <= 0) return cudaSuccess;
+    if (p.pair_chunks == nullptr) return cudaErrorInvalidValue;
     const size_t smem = learned_smem_bytes(max_N, p.warps);
     cudaError_t e = cudaFuncSetAttribute(learned_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

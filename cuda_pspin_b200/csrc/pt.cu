@@ -171,6 +171,42 @@ cudaError_t launch_exchange(const ExchangeParams& p, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------
+// Observable series: one warp per sample.  E of the nrep replicas at the
+// slot and q_ab = Re sum_k a_k^a conj(a_k^b) / N for every pair a < b
+// (the overlap of analysis_pt.cpp:1404-1416), summed in FP64.
+// ---------------------------------------------------------------------
+__global__ void observe_kernel(const ObserveParams P) {
+    const int s = blockIdx.x, lane = threadIdx.x;
+    const long long row = (*P.sweep_counter - P.sweep0) / P.pt_freq - 1;
+    if (s >= P.n_samples || row < 0 || row >= P.capacity) return;
+    const SampleDev S = P.samples[s];
+    const int nr = P.nrep;
+    const int npairs = nr * (nr - 1) / 2;
+    const int* perm = P.perm + ((int64_t)s * P.NT + P.temp_index) * nr;
+    const int64_t base = row * P.n_samples + s;
+    for (int r = lane; r < nr; r += 32) P.E_out[base * nr + r] = P.energy[S.rep_off + perm[r]];
+    int pr = 0;
+    for (int a = 0; a < nr; a++)
+        for (int b = a + 1; b < nr; b++, pr++) {
+            const float2* xa = P.spins + S.spin_off + perm[a];
+            const float2* xb = P.spins + S.spin_off + perm[b];
+            double acc = 0.0;
+            for (int k = lane; k < S.N; k += 32) {
+                const float2 u = xa[(int64_t)k * S.R], v = xb[(int64_t)k * S.R];
+                acc += (double)u.x * v.x + (double)u.y * v.y;
+            }
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if (lane == 0) P.q_out[base * npairs + pr] = acc / S.N;
+        }
+}
+
+cudaError_t launch_observe(const ObserveParams& p, cudaStream_t st) {
+    if (p.n_samples <= 0) return cudaSuccess;
+    observe_kernel<<<p.n_samples, 32, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------
 // FP32 FMA throughput probe: 8 independent register chains per thread, so
 // the FMA pipe, not latency, is the limit.
 // ---------------------------------------------------------------------

@@ -73,11 +73,12 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepParams P) {
     const int steps = N / 2;
     const int total = P.nsweeps * steps;
 
-    Stream st;
+    Stream<2> st;
     st.key0 = S.pair_key0;
     st.key1 = S.pair_key1;
     st.N = N;
     st.site_chunks = P.site_chunks + S.split_off;
+    st.pair_chunks = nullptr;
     st.sweep0 = sweep0;
     st.steps = steps;
     st.total = total;

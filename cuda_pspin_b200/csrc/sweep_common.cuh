@@ -97,19 +97,23 @@ struct Cursor {
     int m, which, c, c_end;
 };
 
+// kLists: lists visited per move -- sites i0, j0 (2); then, for the two-pass
+// sweep, the pair's two sub-lists (4)
+template <int kLists>
 struct Stream {
     uint32_t key0, key1;
     int N;
     const int* site_chunks;   // this sample's N*(kSplit+1) absolute chunk indices
+    const int* pair_chunks;   // this sample's N(N-1)*(kSplit+1) pair sub-list chunk indices
     long long sweep0;
     int steps, total, part0, part1;
-    int lists = 2;            // lists visited per move: i0, j0 (x2 for two field passes)
 
     __device__ __forceinline__ void range(int m, int which, int& c, int& c_end) const {
         int i0, j0;
         const long long sw = sweep0 + m / steps;
         pair_pick(key0, key1, (uint64_t)sw, (uint32_t)(m % steps), N, i0, j0);
-        const int* sc = site_chunks + ((which & 1) ? j0 : i0) * (kSplit + 1);
+        const int* sc = (kLists == 2 || which < 2) ? site_chunks + ((which & 1) ? j0 : i0) * (kSplit + 1)
+                                                   : pair_chunks + (2 * (j0 * (j0 - 1) / 2 + i0) + (which & 1)) * (kSplit + 1);
         c = __ldg(sc + part0);
         c_end = __ldg(sc + part1);
     }
@@ -117,7 +121,7 @@ struct Stream {
     __device__ __forceinline__ void next(Cursor& k) const {
         k.c++;
         while (k.c >= k.c_end) {
-            if (++k.which == lists) {
+            if (++k.which == kLists) {
                 k.which = 0;
                 if (++k.m >= total) return;
             }

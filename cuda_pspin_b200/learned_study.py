@@ -1,0 +1,155 @@
+"""Learned proposal against the plain move: tau_int-corrected throughput at
+one temperature of a PT run.
+
+Workload (dense spherical, FMC uniform omega_i ~ U[0,1), gamma = 0.1):
+S disorder samples (seeds seed0..seed0+S-1) of N sites, NT temperatures
+geometric in [Tmin, Tmax], nrep replicas per temperature, exchange every
+sweep.  Steps:
+
+1. plain PT for `train_sweeps` sweeps with fields at both ends of every
+   move; accepted moves are recorded (probability record_prob) into a ring;
+2. the network is trained on the GPU (own forward/backward/Adam kernels);
+3. `measure_sweeps` sweeps of plain PT, then of PT with the learned move
+   (exact MH), then of plain PT again, each recording E and the pair
+   overlaps q of the replicas at temperature slot `slot` after every sweep.
+   The two plain phases bracket the learned one, so a drift of <E> (an
+   unequilibrated start) shows as a difference between them.
+
+Reported per phase: tau_int of E, of q and of q^2 (Sokal windowing, chains =
+samples x replicas or samples x pairs), wall time, <E>/N at the slot with its
+tau-corrected error, and independent samples per second.  T = 0.3 is not on
+the 24-point grid in [0.2, 1.6]; the nearest slot is 19 (T = 0.28714).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+
+import numpy as np
+
+from . import Engine, PSPIN_DENSE, PROPOSAL_LEARNED, PROPOSAL_PLAIN, PROPOSAL_PLAIN_FIELDS
+from . import default_config, make_options, temperature_schedule
+from . import tau as T
+
+
+def build(args) -> tuple[Engine, np.ndarray]:
+    cfgs = []
+    for k in range(args.samples):
+        c = default_config(N=args.N, nrep=args.NT * args.nrep, seed=args.seed0 + k, fmc_mode=2)
+        c.gamma = args.gamma
+        cfgs.append(c)
+    eng = Engine(cfgs, PSPIN_DENSE, make_options(quiet=True))
+    temps, betas = temperature_schedule(args.NT, args.Tmin, args.Tmax, True)
+    eng.pt_init(args.NT, args.nrep, betas, 1)
+    return eng, temps
+
+
+def run_pt(eng: Engine, sweeps: int, chunk: int = 256) -> float:
+    t0 = time.perf_counter()
+    left = sweeps
+    while left > 0:
+        eng.pt_run(min(chunk, left))
+        left -= min(chunk, left)
+    return time.perf_counter() - t0
+
+
+def measure(eng: Engine, proposal: int, sweeps: int, slot: int, N: int) -> dict:
+    eng.set_proposal(proposal)
+    eng.observe_init(slot, sweeps)
+    eng.reset_counters()
+    seconds = run_pt(eng, sweeps)
+    E, q = eng.observe_get()                                   # [n, S, nrep], [n, S, npairs]
+    _, acc, prop = eng.get_results()
+    e = E.reshape(E.shape[0], -1).T / N                        # chains x n
+    qq = q.reshape(q.shape[0], -1).T
+    te, tq, tq2 = T.tau_int(e), T.tau_int(qq), T.tau_int(qq ** 2)
+    half = e.shape[1] // 2
+    return {
+        "proposal": {PROPOSAL_PLAIN: "plain", PROPOSAL_LEARNED: "learned"}[proposal],
+        "sweeps": sweeps, "seconds": seconds, "sweeps_per_s": sweeps / seconds,
+        "acceptance_all_T": float(acc.sum() / max(prop.sum(), 1)),
+        "E_per_N": float(e.mean()), "E_per_N_err": float(np.sqrt(2.0 * te.tau * e.var() / e.size)),
+        "E_per_N_halves": [float(e[:, :half].mean()), float(e[:, half:].mean())],
+        "tau_E": te.tau, "tau_E_err": te.err, "tau_E_window": te.window,
+        "tau_q": tq.tau, "tau_q_err": tq.err, "tau_q2": tq2.tau, "tau_q2_err": tq2.err,
+        "indep_E_per_s": T.independent_samples_per_second(te, seconds),
+        "indep_q_per_s": T.independent_samples_per_second(tq, seconds),
+        "indep_q2_per_s": T.independent_samples_per_second(tq2, seconds),
+        "q2": float((qq ** 2).mean()),
+    }
+
+
+def run(args) -> dict:
+    eng, temps = build(args)
+    out = {"workload": {"N": args.N, "samples": args.samples, "NT": args.NT, "nrep": args.nrep,
+                        "gamma": args.gamma, "Tmin": args.Tmin, "Tmax": args.Tmax, "slot": args.slot,
+                        "T_slot": float(temps[args.slot]), "train_sweeps": args.train_sweeps,
+                        "measure_sweeps": args.measure_sweeps, "seed0": args.seed0}}
+    eng.learn_init(seed=args.net_seed, capacity=args.capacity, record_prob=args.record_prob)
+    eng.set_proposal(PROPOSAL_PLAIN_FIELDS)
+    t_rec = run_pt(eng, args.train_sweeps)
+    n_rec, _ = eng.learn_records(0)
+    t0 = time.perf_counter()
+    loss0 = eng.learn_train(1, args.batch, 0.0)
+    losses = []
+    for k in range(args.train_steps // 100):
+        lr = args.lr * (0.5 ** (3.0 * k * 100 / max(args.train_steps, 1)))
+        losses.append(eng.learn_train(100, args.batch, lr))
+    t_train = time.perf_counter() - t0
+    out["training"] = {"records_seen": int(n_rec), "record_sweeps_s": t_rec, "train_s": t_train,
+                       "steps": args.train_steps, "batch": args.batch, "loss_start": loss0,
+                       "loss_end": losses[-1] if losses else loss0,
+                       "loss_curve": losses[::max(1, len(losses) // 10)]}
+    if args.equilibrate:
+        eng.set_proposal(PROPOSAL_PLAIN)
+        out["training"]["extra_equilibration_sweeps"] = args.equilibrate
+        run_pt(eng, args.equilibrate)
+    p1 = measure(eng, PROPOSAL_PLAIN, args.measure_sweeps, args.slot, args.N)
+    l = measure(eng, PROPOSAL_LEARNED, args.measure_sweeps, args.slot, args.N)
+    p2 = measure(eng, PROPOSAL_PLAIN, args.measure_sweeps, args.slot, args.N)
+    out["plain"], out["learned"], out["plain_after"] = p1, l, p2
+    for key in ("E", "q", "q2"):
+        plain_rate = 0.5 * (p1[f"indep_{key}_per_s"] + p2[f"indep_{key}_per_s"])
+        out[f"gain_{key}"] = l[f"indep_{key}_per_s"] / plain_rate
+    ep = 0.5 * (p1["E_per_N"] + p2["E_per_N"])
+    sp = 0.5 * np.hypot(p1["E_per_N_err"], p2["E_per_N_err"])
+    out["E_diff_sigma"] = (l["E_per_N"] - ep) / np.hypot(l["E_per_N_err"], sp)
+    out["plain_drift_sigma"] = (p2["E_per_N"] - p1["E_per_N"]) / np.hypot(p1["E_per_N_err"], p2["E_per_N_err"])
+    eng.free()
+    return out
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--N", type=int, default=64)
+    ap.add_argument("--samples", type=int, default=64)
+    ap.add_argument("--NT", type=int, default=24)
+    ap.add_argument("--nrep", type=int, default=4)
+    ap.add_argument("--gamma", type=float, default=0.1)
+    ap.add_argument("--Tmin", type=float, default=0.2)
+    ap.add_argument("--Tmax", type=float, default=1.6)
+    ap.add_argument("--slot", type=int, default=19)
+    ap.add_argument("--seed0", type=int, default=42)
+    ap.add_argument("--train-sweeps", type=int, default=1 << 14)
+    ap.add_argument("--equilibrate", type=int, default=0, help="plain PT sweeps between training and measuring")
+    ap.add_argument("--measure-sweeps", type=int, default=1 << 14)
+    ap.add_argument("--capacity", type=int, default=1 << 22)
+    ap.add_argument("--record-prob", type=float, default=0.01)
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--net-seed", type=int, default=1)
+    ap.add_argument("--out", default="")
+    args = ap.parse_args(argv)
+    res = run(args)
+    print(json.dumps(res))
+    if args.out:
+        with open(args.out, "w") as f:
+            f.write(json.dumps(res, indent=1) + "\n")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -155,6 +155,18 @@ int  pspin_pt_run(pspin_state* s, int nsweeps);
  * cumulative exchange counters [NT-1] of one sample. */
 int  pspin_pt_get(pspin_state* s, int sample, int32_t* perm, int64_t* ex_acc, int64_t* ex_prop);
 int  pspin_pt_sweeps_done(pspin_state* s, int64_t* sweeps);
+/* Observable series at one temperature slot (no reference counterpart; the
+ * reference writes E every save_freq sweeps to energy_accept.txt and
+ * configurations to configs.bin, parallel_tempering.cu:355-416).  After
+ * every exchange step of pspin_pt_run, for every sample: the energies of the
+ * nrep replicas at slot temp_index and the overlaps
+ * q_ab = Re sum_k a_k^a conj(a_k^b) / N of their nrep(nrep-1)/2 pairs
+ * (a < b in slot order).  The first `capacity` steps after the call are
+ * kept; capacity 0 switches recording off. */
+int  pspin_observe_init(pspin_state* s, int temp_index, int capacity);
+/* n_rows: steps recorded (<= capacity); energy [max_rows][S][nrep] and
+ * overlap [max_rows][S][nrep(nrep-1)/2] (either may be NULL). */
+int  pspin_observe_get(pspin_state* s, int64_t* n_rows, double* energy, double* overlap, int max_rows);
 
 /* ---- all-site local fields (no reference counterpart) ----------------- */
 enum { PSPIN_FIELDS_FP64 = 0,      /* FP64 sum over the quartet table */

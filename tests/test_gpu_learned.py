@@ -261,3 +261,67 @@ def test_proposal_state_errors(ps):
         eng.learn_init(seed=1, capacity=8)
         with pytest.raises(ps.PspinError):
             eng.set_proposal(ps.PROPOSAL_PLAIN_FIELDS)     # dense only
+
+
+def test_observer_series_matches_state(ps):
+    """The device series at a slot equals E and q read back from the engine."""
+    N, NT, nr = 12, 4, 3
+    cfgs = [ps.default_config(N=N, nrep=NT * nr, seed=30 + k, fmc_mode=0) for k in range(3)]
+    T, beta = ps.temperature_schedule(NT, 0.4, 1.2, True)
+    with ps.Engine(cfgs) as eng:
+        eng.pt_init(NT, nr, beta, 1)
+        eng.pt_run(5)
+        eng.observe_init(2, 8)
+        for step in range(3):
+            eng.pt_run(1)
+            E, q = eng.observe_get()
+            assert E.shape == (step + 1, 3, nr) and q.shape == (step + 1, 3, 3)
+            Eall, _, _ = eng.get_results()
+            spins = eng.get_spins()
+            for k in range(3):
+                perm, _, _ = eng.pt_get(k)
+                reps = perm[2 * nr:3 * nr]
+                np.testing.assert_array_equal(E[step, k], Eall[k * NT * nr + reps])
+                a = spins[k][reps]
+                qq = [np.real(np.sum(a[x] * np.conj(a[y]))) / N for x in range(nr) for y in range(x + 1, nr)]
+                np.testing.assert_allclose(q[step, k], qq, rtol=0, atol=1e-12)
+        eng.pt_run(10)
+        E, q = eng.observe_get()
+        assert E.shape[0] == 8                       # capacity reached, recording stops
+
+
+def _energy_series(ps, c, proposal, trained_w, nsweeps, burn):
+    from cuda_pspin_b200 import tau as T
+    with ps.Engine(c, ps.PSPIN_DENSE, ps.make_options(resync_every=256)) as eng:
+        eng.learn_init(seed=1, capacity=16)
+        if trained_w is not None:
+            eng.learn_params(trained_w)
+        eng.set_proposal(proposal)
+        eng.fill_betas(1.0 / c.T)
+        eng.sweep(burn)
+        xs = []
+        for _ in range(nsweeps):
+            eng.sweep(1)
+            xs.append(eng.get_results()[0].copy())
+    x = np.array(xs).T / c.N                       # chains x n
+    t = T.tau_int(x)
+    return x.mean(), np.sqrt(2 * t.tau * x.var() / x.size), t.tau
+
+
+@pytest.mark.parametrize("T_", [0.4, 1.0])
+def test_learned_chain_matches_plain_energy(ps, T_):
+    """<E>/N of a trained learned chain equals the plain chain's (beta > 0)."""
+    N = 8
+    c = ps.default_config(N=N, nrep=256, seed=13, fmc_mode=0, T=T_)
+    with ps.Engine(c) as eng:
+        eng.learn_init(seed=2, capacity=1 << 16, record_prob=0.5)
+        eng.set_proposal(ps.PROPOSAL_PLAIN_FIELDS)
+        eng.fill_betas(1.0 / T_)
+        eng.sweep(300)
+        eng.learn_train(400, 4096, 3e-3)
+        w = eng.learn_params()
+    ep, sp, tp = _energy_series(ps, c, ps.PROPOSAL_PLAIN, None, 1500, 300)
+    el, sl, tl = _energy_series(ps, c, ps.PROPOSAL_LEARNED, w, 1500, 300)
+    z = (el - ep) / np.hypot(sp, sl)
+    print(f"T={T_} plain {ep:.5f}+-{sp:.5f} tau {tp:.2f}  learned {el:.5f}+-{sl:.5f} tau {tl:.2f}  z={z:.2f}")
+    assert abs(z) < 4.0
