@@ -27,6 +27,8 @@ PSPIN_DENSE = 0
 PSPIN_SPARSE = 1
 FIELDS_FP64 = 0
 FIELDS_TC_BF16X3 = 1
+RESYNC_FP64 = 0
+RESYNC_TC = 1
 PROPOSAL_PLAIN = 0
 PROPOSAL_PLAIN_FIELDS = 1
 PROPOSAL_LEARNED = 2
@@ -58,7 +60,8 @@ class Options(ctypes.Structure):
     _fields_ = [("init_exact", ctypes.c_int), ("resync_every", ctypes.c_int),
                 ("warps_per_unit", ctypes.c_int), ("trace_sample", ctypes.c_int),
                 ("trace_replica", ctypes.c_int), ("trace_capacity", ctypes.c_int),
-                ("quiet", ctypes.c_int), ("generic_lists", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+                ("quiet", ctypes.c_int), ("generic_lists", ctypes.c_int), ("graph_steps", ctypes.c_int),
+                ("resync_method", ctypes.c_int), ("cluster_size", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
 
 
 class Info(ctypes.Structure):
@@ -117,6 +120,8 @@ def load_library() -> ctypes.CDLL:
         "pspin_local_fields": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp, vp]),
         "pspin_set_proposal": (ctypes.c_int, [vp, ctypes.c_int]),
         "pspin_observe_init": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+        "pspin_autotune": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp]),
+        "pspin_resync_drift": (ctypes.c_int, [vp, vp]),
         "pspin_observe_get": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int]),
         "pspin_learn_init": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_float]),
         "pspin_learn_params": (ctypes.c_int, [vp, vp, vp]),
@@ -168,9 +173,13 @@ def parse_args(argv: list[str]) -> SimConfig:
 
 def make_options(init_exact: bool = False, resync_every: int = 0, warps_per_unit: int = 0,
                  trace: tuple[int, int, int] | None = None, quiet: bool = True,
-                 generic_lists: bool = False) -> Options:
+                 generic_lists: bool = False, graph_steps: int = 0, resync_method: int = 0,
+                 cluster_size: int = 0) -> Options:
     o = Options()
+    o.cluster_size = int(cluster_size)
+    o.resync_method = int(resync_method)
     o.generic_lists = int(generic_lists)
+    o.graph_steps = int(graph_steps)
     o.init_exact = int(init_exact)
     o.resync_every = resync_every
     o.warps_per_unit = warps_per_unit
@@ -317,6 +326,19 @@ class Engine:
         prop = np.empty(NT - 1, np.int64)
         _check(self._lib.pspin_pt_get(self._h, sample, _ptr(perm), _ptr(acc), _ptr(prop)))
         return perm, acc, prop
+
+    def resync_drift(self) -> np.ndarray:
+        """|E_running - E_recomputed| per replica at the last periodic resync."""
+        d = np.empty(self.n_replicas, np.float64)
+        _check(self._lib.pspin_resync_drift(self._h, _ptr(d)))
+        return d
+
+    def autotune(self, sweeps: int = 8):
+        """(warps per CTA, CTAs per replica block, ms per sweep [cluster 1,2,4,8,16][warps 1,2,4,8])."""
+        w, c = ctypes.c_int(0), ctypes.c_int(0)
+        ms = np.zeros((5, 4), np.float32)
+        _check(self._lib.pspin_autotune(self._h, int(sweeps), ctypes.byref(w), ctypes.byref(c), _ptr(ms)))
+        return w.value, c.value, ms
 
     def observe_init(self, temp_index: int, capacity: int) -> None:
         _check(self._lib.pspin_observe_init(self._h, int(temp_index), int(capacity)))

@@ -1,0 +1,151 @@
+"""The engine on the benchmark configurations beside the reference's sm_100a
+rebuild (its numbers, when present, from profiles/reference_sm100_timing.json,
+written by tests/golden/time_reference.py on the same kind of GPU).
+
+  1  dense spherical PT, N=32, FMC uniform gamma=0.1, NT=20 geometric in
+     [0.2, 1.6], nrep 4, seed 42 (one sample)
+  2  sparse cube PT, N=512, FMC comb gamma=1, NT=32, nrep 4, seed 42
+  4  dense spherical MC, N=128 fully connected, 64 replicas at T=0.5
+  5  dense spherical PT, N=64, FMC uniform gamma=0.1, NT=24, nrep 4:
+     one sample (seed 42, the reference's run) and 64 samples (seeds 42..105)
+(3, the batched workload, is bench.py's.)
+
+Each run: set-up, a few warm-up sweeps, the block-shape autotuner, then a
+timed run of device-resident sweeps (PT cycles replayed as CUDA graphs) with
+the wall clock around the synchronous calls.  Rate = replicas x N/2 x sweeps
+/ seconds (pair-moves/s), the reference's unit.
+
+--precision runs configuration 4 for 2^12 sweeps with the running energy
+resynchronised every 256 sweeps from the split-BF16 tensor-core contraction
+and reports, per resync, the FP32 accumulation drift and, at the end, the
+running and tensor-core energies against the FP64 energies of the same
+amplitudes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+from . import (Engine, PSPIN_DENSE, PSPIN_SPARSE, RESYNC_TC, FIELDS_TC_BF16X3, default_config, make_options,
+               temperature_schedule)
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_KEYS = {"1": "config1_dense_pt_n32_fmc2", "2": "config2_sparse_pt_n512_comb", "4": "config4_dense_mc_n128",
+            "5": "config5_dense_pt_n64_fmc2"}
+
+
+def _pt_engine(N, seeds, NT, nrep, variant, fmc, gamma, Tmin=0.2, Tmax=1.6):
+    cfgs = []
+    for s in seeds:
+        c = default_config(N=N, nrep=NT * nrep, seed=s, fmc_mode=fmc)
+        c.gamma = gamma
+        cfgs.append(c)
+    t0 = time.perf_counter()
+    eng = Engine(cfgs, variant, make_options(quiet=True))
+    setup = time.perf_counter() - t0
+    _, betas = temperature_schedule(NT, Tmin, Tmax, True)
+    eng.pt_init(NT, nrep, betas, 1)
+    return eng, setup
+
+
+def _timed(eng, run, sweeps, warmup, tune_sweeps):
+    run(warmup)
+    w, c, ms = eng.autotune(tune_sweeps)
+    run(warmup)
+    t0 = time.perf_counter()
+    run(sweeps)
+    return time.perf_counter() - t0, w, c
+
+
+def measure(config: str, sweeps: int | None = None) -> dict:
+    if config == "1":
+        eng, setup = _pt_engine(32, [42], 20, 4, PSPIN_DENSE, 2, 0.1)
+        sweeps = sweeps or 4096
+        run = eng.pt_run
+    elif config == "2":
+        eng, setup = _pt_engine(512, [42], 32, 4, PSPIN_SPARSE, 1, 1.0)
+        sweeps = sweeps or 4096
+        run = eng.pt_run
+    elif config == "4":
+        c = default_config(N=128, nrep=64, seed=42, fmc_mode=0, T=0.5)
+        t0 = time.perf_counter()
+        eng = Engine(c, PSPIN_DENSE, make_options(quiet=True))
+        setup = time.perf_counter() - t0
+        eng.fill_betas(2.0)
+        sweeps = sweeps or 64
+        run = eng.sweep
+    elif config == "5":
+        eng, setup = _pt_engine(64, [42], 24, 4, PSPIN_DENSE, 2, 0.1)
+        sweeps = sweeps or 2048
+        run = eng.pt_run
+    elif config == "5x64":
+        eng, setup = _pt_engine(64, list(range(42, 106)), 24, 4, PSPIN_DENSE, 2, 0.1)
+        sweeps = sweeps or 1024
+        run = eng.pt_run
+    else:
+        raise ValueError(config)
+    moves = sum(N * R // 2 for N, R in zip(eng.Ns, eng.Rs))
+    secs, w, cl = _timed(eng, run, sweeps, warmup=8, tune_sweeps=2 if config == "4" else 8)
+    eng.free()
+    out = {"config": config, "sweeps": sweeps, "seconds": secs, "pair_moves_per_s": moves * sweeps / secs,
+           "warps_per_cta": w, "ctas_per_replica_block": cl, "setup_s": setup}
+    ref = os.path.join(ROOT, "profiles", "reference_sm100_timing.json")
+    key = REF_KEYS.get(config)
+    if key and os.path.exists(ref):
+        r = json.load(open(ref)).get(key)
+        if r:
+            out["reference_pair_moves_per_s"] = r["pair_moves_per_s"]
+            out["speedup_vs_reference"] = out["pair_moves_per_s"] / r["pair_moves_per_s"]
+    return out
+
+
+def precision(sweeps: int = 1 << 12, every: int = 256) -> dict:
+    c = default_config(N=128, nrep=64, seed=42, fmc_mode=0, T=0.5)
+    eng = Engine(c, PSPIN_DENSE, make_options(quiet=True, resync_every=every, resync_method=RESYNC_TC))
+    eng.fill_betas(2.0)
+    w, cl, _ = eng.autotune(2)
+    drifts = []
+    t0 = time.perf_counter()
+    for _ in range(sweeps // every):
+        eng.sweep(every)                       # ends on a resync
+        drifts.append(float(eng.resync_drift().max() / c.N))
+    secs = time.perf_counter() - t0
+    E_run, _, _ = eng.get_results()
+    e2, e4 = eng.split_energies()            # FP64, same amplitudes
+    E64 = e2 + e4
+    _, E_tc = eng.local_fields(0, FIELDS_TC_BF16X3)
+    eng.free()
+    rel = lambda a: float(np.max(np.abs(a - E64) / np.abs(E64)))
+    return {"config": "4-precision", "sweeps": sweeps, "resync_every": every, "seconds": secs,
+            "warps_per_cta": w, "ctas_per_replica_block": cl,
+            "max_fp32_drift_per_site_between_resyncs": drifts,
+            "final_E_per_site_fp64_mean": float(E64.mean() / c.N),
+            "final_running_vs_fp64_max_rel": rel(E_run), "final_tc_vs_fp64_max_rel": rel(np.asarray(E_tc)),
+            "final_running_vs_fp64_max_abs_per_site": float(np.max(np.abs(E_run - E64)) / c.N)}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--configs", default="1,2,4,5,5x64")
+    ap.add_argument("--precision", action="store_true")
+    ap.add_argument("--out", default="")
+    a = ap.parse_args(argv)
+    res = [measure(k) for k in a.configs.split(",") if k]
+    if a.precision:
+        res.append(precision())
+    for r in res:
+        print(json.dumps(r))
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(res, f, indent=1)
+            f.write("\n")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

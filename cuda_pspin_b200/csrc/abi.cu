@@ -44,6 +44,7 @@ struct LearnParams {
     float rec_prob;
 };
 cudaError_t launch_learned_sweep(const SweepParams& p, const LearnParams& l, int n_units, int max_N, cudaStream_t st);
+size_t learned_smem_bytes_host(int N, int warps);
 cudaError_t launch_mlp_fwd_bwd(const float* w, const float* records, const int* index, int n, float* save,
                                float* loss, cudaStream_t st);
 cudaError_t launch_mlp_grad(const float* save, int n, float* grad, cudaStream_t st);
@@ -139,7 +140,7 @@ struct pspin_state {
     std::vector<SampleHost> hs;
     std::vector<SampleDev> sd;
     std::vector<Unit> units;
-    int R_tot = 0, max_N = 0, warps = 8;
+    int R_tot = 0, max_N = 0, warps = 8, cluster = 1;
     int64_t spin_total = 0;
     cudaStream_t st = nullptr;
     int device = 0;
@@ -207,6 +208,12 @@ struct pspin_state {
     long long sweeps_done = 0;
     long long since_resync = 0;
 
+    // CUDA graph of graph_G PT steps (pspin_pt_run), rebuilt when a captured
+    // pointer or kernel choice changes
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_G = 0;
+    long long graph_launches = 0;
+
     // measurement
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
@@ -216,6 +223,7 @@ struct pspin_state {
 
 static void free_state(pspin_state* s) {
     if (!s) return;
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
     void* ptrs[] = {s->d_samples, s->d_units, s->d_spins, s->d_E, s->d_beta, s->d_target, s->d_drift,
                     s->d_e2, s->d_e4, s->d_acc, s->d_prop, s->d_key, s->d_entries, s->d_chunk_start, s->d_site_chunks,
                     s->d_q64, s->d_g2, s->d_g4re, s->d_mask, s->d_sweep_counter, s->d_status,
@@ -712,6 +720,15 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         s->opt.trace_replica = -1;
     }
     if (s->opt.resync_every == 0) s->opt.resync_every = 1024;
+    if (s->opt.resync_method != PSPIN_RESYNC_FP64 && s->opt.resync_method != PSPIN_RESYNC_TC) {
+        const int m = s->opt.resync_method;
+        delete s;
+        return fail(PSPIN_ERR_ARG, "unknown resync method %d", m);
+    }
+    if (s->opt.resync_method == PSPIN_RESYNC_TC && (variant != PSPIN_DENSE || n != 1)) {
+        delete s;
+        return fail(PSPIN_ERR_UNSUPPORTED, "the tensor-core resync takes one dense sample per handle");
+    }
     s->variant = variant;
     s->S = n;
     s->hs.resize(n);
@@ -920,6 +937,13 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     });
     s->warps = choose_warps(s);
     if (s->warps < 0) return bail(fail(PSPIN_ERR_ARG, "warps_per_unit must be 1, 2, 4 or 8"));
+    {
+        const int c = s->opt.cluster_size == 0 ? 1 : s->opt.cluster_size;
+        if (c != 1 && c != 2 && c != 4 && c != 8 && c != 16)
+            return bail(fail(PSPIN_ERR_ARG, "cluster_size must be 1, 2, 4, 8 or 16"));
+        if (c * s->warps > kSplit) return bail(fail(PSPIN_ERR_ARG, "cluster_size * warps_per_unit must be <= 32"));
+        s->cluster = c;
+    }
     if (sweep_smem_bytes(s->max_N, s->warps) > 227 * 1024)
         return bail(fail(PSPIN_ERR_ARG, "N=%d needs more shared memory than a CTA has", s->max_N));
 
@@ -960,6 +984,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         cudaError_t e = cudaMemsetAsync(s->d_acc, 0, s->R_tot * sizeof(long long), s->st);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->d_prop, 0, s->R_tot * sizeof(long long), s->st);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->d_E, 0, s->R_tot * sizeof(double), s->st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->d_drift, 0, s->R_tot * sizeof(double), s->st);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->d_sweep_counter, 0, sizeof(long long), s->st);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->d_status, 0, sizeof(int), s->st);
         if (e != cudaSuccess) return bail(fail(PSPIN_ERR_CUDA, "memset: %s", cudaGetErrorString(e)));
@@ -996,7 +1021,11 @@ extern "C" int pspin_total_replicas(const pspin_state* s) { return s ? s->R_tot 
 extern "C" int pspin_num_samples(const pspin_state* s) { return s ? s->S : 0; }
 
 // ------------------------------------------------------------------ sweeps
-static int launch_chunk(pspin_state* s, int nsweeps, bool exchange) {
+// Enqueues one step: a sweep launch of nsweeps sweeps, the exchange launch
+// (which advances the device sweep counter) and, after an exchange, the
+// observable recorder.  No host bookkeeping, so a sequence of steps can be
+// captured in a CUDA graph; e0/e1 (optional) bracket the sweep kernel.
+static int enqueue_step(pspin_state* s, int nsweeps, bool exchange, cudaEvent_t e0, cudaEvent_t e1) {
     SweepParams p{};
     p.samples = s->d_samples;
     p.units = s->d_units;
@@ -1019,20 +1048,11 @@ static int launch_chunk(pspin_state* s, int nsweeps, bool exchange) {
     p.trace_sweep0 = s->trace_sweep0;
     p.trace = s->d_trace;
     p.status = s->d_status;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (s->profiling) {
-        if (s->ev_used == s->ev_pool.size()) {
-            std::pair<cudaEvent_t, cudaEvent_t> pr;
-            CK(cudaEventCreate(&pr.first));
-            CK(cudaEventCreate(&pr.second));
-            s->ev_pool.push_back(pr);
-        }
-        e0 = s->ev_pool[s->ev_used].first;
-        e1 = s->ev_pool[s->ev_used].second;
-        s->ev_used++;
-        CK(cudaEventRecord(e0, s->st));
-    }
-    if (s->proposal == PSPIN_PROPOSAL_PLAIN) {
+    if (e0) CK(cudaEventRecord(e0, s->st));
+    p.cluster = s->proposal == PSPIN_PROPOSAL_PLAIN ? s->cluster : 1;
+    if (s->proposal == PSPIN_PROPOSAL_PLAIN && s->cluster > 1) {
+        CK(launch_sweep_cluster(p, (int)s->units.size(), s->variant, s->max_N, s->st, nullptr));
+    } else if (s->proposal == PSPIN_PROPOSAL_PLAIN) {
         CK(launch_sweep(p, (int)s->units.size(), s->variant, s->max_N, s->st));
     } else {
         LearnParams lp{};
@@ -1044,9 +1064,7 @@ static int launch_chunk(pspin_state* s, int nsweeps, bool exchange) {
         lp.rec_prob = s->rec_prob;
         CK(launch_learned_sweep(p, lp, (int)s->units.size(), s->max_N, s->st));
     }
-    if (s->profiling) CK(cudaEventRecord(e1, s->st));
-    s->sweep_launches++;
-    s->kernel_launches++;
+    if (e1) CK(cudaEventRecord(e1, s->st));
     ExchangeParams x{};
     x.n_samples = s->S;
     x.NT = s->pt_NT;
@@ -1063,7 +1081,6 @@ static int launch_chunk(pspin_state* s, int nsweeps, bool exchange) {
     x.nsweeps_done = nsweeps;
     x.do_exchange = exchange ? 1 : 0;
     CK(launch_exchange(x, s->st));
-    s->kernel_launches++;
     if (exchange && s->obs_cap > 0) {
         ObserveParams o{};
         o.n_samples = s->S;
@@ -1081,22 +1098,100 @@ static int launch_chunk(pspin_state* s, int nsweeps, bool exchange) {
         o.E_out = s->d_obs_E;
         o.q_out = s->d_obs_q;
         CK(launch_observe(o, s->st));
-        s->kernel_launches++;
     }
-    s->sweeps_done += nsweeps;
-    s->since_resync += nsweeps;
+    return PSPIN_OK;
+}
+
+static int do_resync(pspin_state* s);
+
+// host counters after `steps` steps of nsweeps sweeps each; the resync when due
+static int account_steps(pspin_state* s, int steps, int nsweeps, bool exchange) {
+    s->sweep_launches += steps;
+    s->kernel_launches += (long long)steps * (2 + ((exchange && s->obs_cap > 0) ? 1 : 0));
+    s->sweeps_done += (long long)steps * nsweeps;
+    s->since_resync += (long long)steps * nsweeps;
     if (s->opt.resync_every > 0 && s->since_resync >= s->opt.resync_every) {
-        TRY(run_energy(s, nullptr, nullptr, true, true));
+        TRY(do_resync(s));
         s->since_resync = 0;
     }
+    return PSPIN_OK;
+}
+
+static int launch_chunk(pspin_state* s, int nsweeps, bool exchange) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (s->profiling) {
+        if (s->ev_used == s->ev_pool.size()) {
+            std::pair<cudaEvent_t, cudaEvent_t> pr;
+            CK(cudaEventCreate(&pr.first));
+            CK(cudaEventCreate(&pr.second));
+            s->ev_pool.push_back(pr);
+        }
+        e0 = s->ev_pool[s->ev_used].first;
+        e1 = s->ev_pool[s->ev_used].second;
+        s->ev_used++;
+    }
+    TRY(enqueue_step(s, nsweeps, exchange, e0, e1));
+    return account_steps(s, 1, nsweeps, exchange);
+}
+
+static void drop_graph(pspin_state* s) {
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    s->graph_exec = nullptr;
+}
+
+static int graph_steps(const pspin_state* s) {
+    const int g = s->opt.graph_steps;
+    return g == 0 ? 32 : (g < 0 ? 0 : g);
+}
+
+// One graph of G PT steps (pt_freq sweeps, exchange, observe), captured on
+// the engine's stream.  The kernels read the sweep index from the device
+// counter that the exchange kernel advances, so every replay continues the
+// same move and pair streams as direct launches would.
+static int capture_graph(pspin_state* s, int G) {
+    drop_graph(s);
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+    int rc = PSPIN_OK;
+    for (int g = 0; g < G && rc == PSPIN_OK; g++) rc = enqueue_step(s, s->pt_freq, true, nullptr, nullptr);
+    cudaError_t e = cudaStreamEndCapture(s->st, &graph);
+    if (rc != PSPIN_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&s->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        s->graph_exec = nullptr;
+        return fail(PSPIN_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    s->graph_G = G;
     return PSPIN_OK;
 }
 
 static int run_sweeps(pspin_state* s, int nsweeps, bool pt) {
     if (!s) return fail(PSPIN_ERR_ARG, "null handle");
     if (nsweeps < 0) return fail(PSPIN_ERR_ARG, "nsweeps < 0");
+    const int G = (pt && !s->profiling) ? graph_steps(s) : 0;
     int left = nsweeps;
     while (left > 0) {
+        // whole graphs of G steps up to the next resync, from a step boundary
+        if (G > 0 && s->sweeps_done % s->pt_freq == 0) {
+            long long room = left;
+            if (s->opt.resync_every > 0) room = std::min<long long>(room, s->opt.resync_every - s->since_resync);
+            const long long reps = room / ((long long)G * s->pt_freq);
+            if (reps > 0) {
+                if (!s->graph_exec || s->graph_G != G) TRY(capture_graph(s, G));
+                for (long long r = 0; r < reps; r++) {
+                    CK(cudaGraphLaunch(s->graph_exec, s->st));
+                    s->graph_launches++;
+                    TRY(account_steps(s, G, s->pt_freq, true));
+                }
+                left -= (int)(reps * G * s->pt_freq);
+                continue;
+            }
+        }
         int chunk = left;
         if (s->opt.resync_every > 0) chunk = std::min<long long>(chunk, s->opt.resync_every - s->since_resync);
         bool ex = false;
@@ -1115,6 +1210,102 @@ static int run_sweeps(pspin_state* s, int nsweeps, bool pt) {
     int status = 0;
     CK(cudaMemcpy(&status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     if (status) return fail(PSPIN_ERR_TIMEOUT, "a bounded wait in the sweep kernel expired (status %d)", status);
+    return PSPIN_OK;
+}
+
+// Whether `cluster` CTAs of `warps` warps can hold one replica block (shared
+// memory, co-residency of the cluster); the plain kernel for cluster 1.
+static bool shape_fits(pspin_state* s, int warps, int cluster) {
+    if (cluster * warps > kSplit) return false;
+    if (s->proposal != PSPIN_PROPOSAL_PLAIN) return cluster == 1 && learned_smem_bytes_host(s->max_N, warps) <= 227 * 1024;
+    if (cluster == 1) return sweep_smem_bytes(s->max_N, warps) <= 227 * 1024;
+    if (cluster_smem_bytes_host(s->max_N, warps, cluster) > 227 * 1024) return false;
+    SweepParams p{};
+    p.warps = warps;
+    p.cluster = cluster;
+    int n = 0;
+    if (launch_sweep_cluster(p, (int)s->units.size(), s->variant, s->max_N, s->st, &n) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return n > 0;
+}
+
+// Times `sweeps` sweeps (no exchange) for every block shape -- CTAs per
+// replica block (cluster) x warps per CTA -- from the same saved state and
+// keeps the fastest.  The state (amplitudes, energies, counters, sweep index)
+// is restored after every trial, so the chain continues as if the trials had
+// not run.
+extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int* chosen_cluster, float* ms_out) {
+    if (!s || sweeps < 1) return fail(PSPIN_ERR_ARG, "bad arguments");
+    float2* b_spins = nullptr;
+    double* b_E = nullptr;
+    long long *b_acc = nullptr, *b_prop = nullptr, *b_cnt = nullptr;
+    int rc;
+    if ((rc = dalloc(&b_spins, (size_t)s->spin_total)) || (rc = dalloc(&b_E, s->R_tot)) ||
+        (rc = dalloc(&b_acc, s->R_tot)) || (rc = dalloc(&b_prop, s->R_tot)) || (rc = dalloc(&b_cnt, 1))) {
+        cudaFree(b_spins); cudaFree(b_E); cudaFree(b_acc); cudaFree(b_prop); cudaFree(b_cnt);
+        return rc;
+    }
+    auto copy_all = [&](bool save) -> cudaError_t {
+        const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+        struct { void* a; void* b; size_t n; } t[] = {
+            {b_spins, s->d_spins, s->spin_total * sizeof(float2)}, {b_E, s->d_E, s->R_tot * sizeof(double)},
+            {b_acc, s->d_acc, s->R_tot * sizeof(long long)}, {b_prop, s->d_prop, s->R_tot * sizeof(long long)},
+            {b_cnt, s->d_sweep_counter, sizeof(long long)}};
+        for (auto& c : t) {
+            cudaError_t e = save ? cudaMemcpyAsync(c.a, c.b, c.n, k, s->st) : cudaMemcpyAsync(c.b, c.a, c.n, k, s->st);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    const int w0 = s->warps, c0 = s->cluster;
+    const float prob0 = s->rec_prob;
+    s->rec_prob = 0.f;                       // trials record no training moves
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaError_t e = copy_all(true);
+    if (e == cudaSuccess) e = cudaEventCreate(&t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&t1);
+    int best_w = w0, best_c = c0;
+    float best_ms = 0.f;
+    const int cw[4] = {1, 2, 4, 8}, cc[5] = {1, 2, 4, 8, 16};
+    for (int ci = 0; ci < 5; ci++)
+        for (int wi = 0; wi < 4; wi++) {
+            float ms = -1.f;
+            if (e == cudaSuccess && rc == PSPIN_OK && shape_fits(s, cw[wi], cc[ci])) {
+                s->warps = cw[wi];
+                s->cluster = cc[ci];
+                rc = enqueue_step(s, 1, false, nullptr, nullptr);          // warm-up sweep
+                if (rc == PSPIN_OK) e = cudaEventRecord(t0, s->st);
+                for (int k = 0; k < sweeps && rc == PSPIN_OK && e == cudaSuccess; k++)
+                    rc = enqueue_step(s, 1, false, nullptr, nullptr);
+                if (rc == PSPIN_OK && e == cudaSuccess) e = cudaEventRecord(t1, s->st);
+                if (rc == PSPIN_OK && e == cudaSuccess) e = cudaEventSynchronize(t1);
+                if (rc == PSPIN_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+                if (rc == PSPIN_OK && e == cudaSuccess) {
+                    ms /= sweeps;
+                    if (best_ms <= 0.f || ms < best_ms) { best_ms = ms; best_w = cw[wi]; best_c = cc[ci]; }
+                }
+                if (e == cudaSuccess) e = copy_all(false);
+            }
+            if (ms_out) ms_out[ci * 4 + wi] = ms;
+        }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    int status = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    cudaFree(b_spins); cudaFree(b_E); cudaFree(b_acc); cudaFree(b_prop); cudaFree(b_cnt);
+    s->rec_prob = prob0;
+    const bool good = rc == PSPIN_OK && e == cudaSuccess;
+    s->warps = good ? best_w : w0;
+    s->cluster = good ? best_c : c0;
+    drop_graph(s);
+    if (rc != PSPIN_OK) return rc;
+    if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+    if (status) return fail(PSPIN_ERR_TIMEOUT, "a bounded wait in the sweep kernel expired (status %d)", status);
+    if (chosen_warps) *chosen_warps = s->warps;
+    if (chosen_cluster) *chosen_cluster = s->cluster;
     return PSPIN_OK;
 }
 
@@ -1258,6 +1449,7 @@ extern "C" int pspin_get_sparse_quartets(pspin_state* s, int sample, int32_t* ij
 extern "C" int pspin_pt_init(pspin_state* s, int NT, int nrep, const double* beta_sched, int pt_freq) {
     if (!s || !beta_sched) return fail(PSPIN_ERR_ARG, "null argument");
     if (NT < 2 || nrep < 1 || pt_freq < 1) return fail(PSPIN_ERR_ARG, "need NT >= 2, nrep >= 1, pt_freq >= 1");
+    drop_graph(s);
     for (const SampleHost& h : s->hs)
         if (h.R != NT * nrep) return fail(PSPIN_ERR_ARG, "sample nrep %d != NT*nrep_per_temp %d", h.R, NT * nrep);
     cudaFree(s->d_beta_sched);
@@ -1315,6 +1507,7 @@ extern "C" int pspin_observe_init(pspin_state* s, int temp_index, int capacity) 
     if (s->pt_NT < 2) return fail(PSPIN_ERR_STATE, "pspin_pt_init has not been called");
     if (temp_index < 0 || temp_index >= s->pt_NT || capacity < 0)
         return fail(PSPIN_ERR_ARG, "temperature index %d outside [0, %d) or negative capacity", temp_index, s->pt_NT);
+    drop_graph(s);
     cudaFree(s->d_obs_E);
     cudaFree(s->d_obs_q);
     s->d_obs_E = nullptr;
@@ -1415,6 +1608,65 @@ static int tc_prepare(pspin_state* s, int sample) {
     return PSPIN_OK;
 }
 
+// All-site fields and energies of one dense sample on the tensor cores:
+// split-BF16 pair operands, the sm100 GEMM, then fields and E2 / E4
+// (d_tc_h [R][N], d_tc_e [E2 of R | E4 of R]), enqueued on the stream.
+static int tc_fields(pspin_state* s, int sample) {
+    const SampleHost& hs = s->hs[sample];
+    const SampleDev& d = s->sd[sample];
+    const int N = hs.N, R = hs.R;
+    const float2* spins = s->d_spins + d.spin_off;
+    TRY(tc_prepare(s, sample));
+    const int npairs = N * (N - 1) / 2;
+    CK(launch_pair_split(spins, N, R, npairs, s->tc_Kp, s->d_tc_x, s->st));
+    CK(tc_gemm(s->tc_M, s->tc_NC, 3 * s->tc_Kp, s->d_tc_w, s->d_tc_x, s->d_tc_f, s->d_tc_ws, s->tc_ws_bytes, s->st,
+               nullptr));
+    CK(launch_site_fields(spins, N, R, s->d_tc_f, s->tc_NC, s->d_g2 + d.g2_off, hs.h2_active, s->d_tc_h, s->d_tc_e,
+                          s->d_tc_e + R, s->st));
+    s->kernel_launches += 3;
+    return PSPIN_OK;
+}
+
+// Periodic resync.  FP64 (default): renormalise, full FP64 energies, running
+// energy overwritten.  Tensor cores (one dense sample): renormalise in FP64,
+// then energies from the split-BF16 contraction.  Both record
+// |E_running - E_recomputed| per replica first.
+static int do_resync(pspin_state* s) {
+    if (s->opt.resync_method != PSPIN_RESYNC_TC) return run_energy(s, nullptr, nullptr, true, true);
+    EnergyParams p{};
+    p.samples = s->d_samples;
+    p.units = s->d_units;
+    p.spins = s->d_spins;
+    p.quartets = s->d_q64;
+    p.g2 = s->d_g2;
+    p.target = s->d_target;
+    p.renorm_only = 1;
+    CK(launch_energy(p, (int)s->units.size(), s->max_N, s->st));
+    s->kernel_launches++;
+    TRY(tc_fields(s, 0));
+    const int R = s->hs[0].R;
+    std::vector<double> run(R), e(2 * (size_t)R), drift(R);
+    CK(cudaMemcpyAsync(run.data(), s->d_E, R * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(e.data(), s->d_tc_e, 2 * R * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (int r = 0; r < R; r++) {
+        const double et = e[r] + e[R + r];
+        drift[r] = std::fabs(run[r] - et);
+        run[r] = et;
+    }
+    CK(cudaMemcpyAsync(s->d_E, run.data(), R * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->d_drift, drift.data(), R * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_resync_drift(pspin_state* s, double* drift) {
+    if (!s || !drift) return fail(PSPIN_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(drift, s->d_drift, s->R_tot * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
 extern "C" int pspin_local_fields(pspin_state* s, int sample, int method, double* h, double* energy) {
     if (!s || !h || sample < 0 || sample >= s->S) return fail(PSPIN_ERR_ARG, "bad arguments");
     if (s->variant != PSPIN_DENSE) return fail(PSPIN_ERR_UNSUPPORTED, "all-site fields: dense variant only");
@@ -1449,14 +1701,7 @@ extern "C" int pspin_local_fields(pspin_state* s, int sample, int method, double
         return PSPIN_OK;
     }
     if (method != PSPIN_FIELDS_TC_BF16X3) return fail(PSPIN_ERR_ARG, "unknown field method %d", method);
-    TRY(tc_prepare(s, sample));
-    const int npairs = N * (N - 1) / 2;
-    CK(launch_pair_split(spins, N, R, npairs, s->tc_Kp, s->d_tc_x, s->st));
-    CK(tc_gemm(s->tc_M, s->tc_NC, 3 * s->tc_Kp, s->d_tc_w, s->d_tc_x, s->d_tc_f, s->d_tc_ws, s->tc_ws_bytes, s->st,
-               nullptr));
-    CK(launch_site_fields(spins, N, R, s->d_tc_f, s->tc_NC, g2, hs.h2_active, s->d_tc_h, s->d_tc_e,
-                          s->d_tc_e + R, s->st));
-    s->kernel_launches += 3;
+    TRY(tc_fields(s, sample));
     std::vector<float2> hv((size_t)R * N);
     CK(cudaMemcpyAsync(hv.data(), s->d_tc_h, hv.size() * sizeof(float2), cudaMemcpyDeviceToHost, s->st));
     CK(cudaMemcpyAsync(e.data(), s->d_tc_e, 2 * R * sizeof(double), cudaMemcpyDeviceToHost, s->st));
@@ -1564,6 +1809,7 @@ extern "C" int pspin_set_proposal(pspin_state* s, int proposal) {
     if (proposal == PSPIN_PROPOSAL_LEARNED && !s->d_wbf)
         return fail(PSPIN_ERR_STATE, "pspin_learn_init has not been called");
     if (proposal != PSPIN_PROPOSAL_PLAIN) TRY(ensure_pair_lists(s));
+    if (proposal != s->proposal) drop_graph(s);
     s->proposal = proposal;
     return PSPIN_OK;
 }
@@ -1571,6 +1817,7 @@ extern "C" int pspin_set_proposal(pspin_state* s, int proposal) {
 extern "C" int pspin_learn_init(pspin_state* s, uint64_t seed, int capacity, float record_prob) {
     if (!s) return fail(PSPIN_ERR_ARG, "null handle");
     if (capacity < 1) return fail(PSPIN_ERR_ARG, "record capacity must be >= 1");
+    drop_graph(s);
     for (void* p : {(void*)s->d_w32, (void*)s->d_adam_m, (void*)s->d_adam_v, (void*)s->d_grad, (void*)s->d_wbf,
                     (void*)s->d_records, (void*)s->d_rec_count})
         if (p) cudaFree(p);

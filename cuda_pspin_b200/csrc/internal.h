@@ -97,6 +97,7 @@ struct SweepParams {
     const long long* sweep_counter;   // global sweep index at launch start
     int nsweeps;
     int warps;                        // warps per unit (divides 32)
+    int cluster;                      // CTAs per unit (sweep_cluster_kernel), 1: sweep_kernel
     // trace
     int trace_sample, trace_rep, trace_cap;
     long long trace_sweep0;
@@ -113,6 +114,9 @@ inline size_t sweep_smem_bytes(int N, int warps) {
 
 // kernels (launchers are host functions in the .cu files)
 cudaError_t launch_sweep(const SweepParams& p, int n_units, int variant, int max_N, cudaStream_t st);
+cudaError_t launch_sweep_cluster(const SweepParams& p, int n_units, int variant, int max_N, cudaStream_t st,
+                                 int* max_clusters);
+size_t cluster_smem_bytes_host(int N, int warps, int C);
 
 struct EnergyParams {
     const SampleDev* samples;
@@ -125,6 +129,7 @@ struct EnergyParams {
     double* energy;           // when non-null: running energy <- e2+e4, drift recorded
     double* drift;            // |E_running - E_fp64| before the overwrite (when energy set)
     const double* target;     // constraint target per replica (renormalise when non-null)
+    int renorm_only;          // 1: renormalise and return (energies come from elsewhere)
 };
 cudaError_t launch_energy(const EnergyParams& p, int n_units, int max_N, cudaStream_t st);
 

@@ -292,11 +292,19 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
                 for (int o = 0; o < kMlpOut; o++) out[o] = outs[o * 32 + lane];
                 ProposalParams pr;
                 decode_outputs(out, pr);
+                // The sampler proposes t' only inside I = (1e-7, 1 - 1e-7), so the
+                // move's density is q_L 1[t' in I]; the reverse move exists only
+                // if the current t is in I as well.  Accepting only then gives
+                // the transition density min(pi q_L, pi' q_L') 1[t in I] 1[t' in I],
+                // symmetric in x and x'.
                 const float t = fmaf(ai.x, ai.x, ai.y * ai.y) / Ssum;
-                const float lq_rev = log_learned_density(pr, t, argf(ai) + argf(hi2), argf(aj) + argf(hj2)) -
-                                     log_plain_density(t);
-                lq_ratio = lq_rev - lq_fwd;
-                accept = ok && (logf(cu) < -beta * dE + lq_ratio);
+                const bool t_in = t > kTEdge && t < 1.0f - kTEdge;
+                if (t_in) {
+                    const float lq_rev = log_learned_density(pr, t, argf(ai) + argf(hi2), argf(aj) + argf(hj2)) -
+                                         log_plain_density(t);
+                    lq_ratio = lq_rev - lq_fwd;
+                }
+                accept = ok && t_in && (logf(cu) < -beta * dE + lq_ratio);
             }
             sp[i0 * kRepBlock + lane] = accept ? ain : ai;
             sp[j0 * kRepBlock + lane] = accept ? ajn : aj;
@@ -344,6 +352,8 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
         P.proposed[gr] += nprop;
     }
 }
+
+size_t learned_smem_bytes_host(int N, int warps) { return learned_smem_bytes(N, warps); }
 
 cudaError_t launch_learned_sweep(const SweepParams& p, const LearnParams& l, int n_units, int max_N,
                                  cudaStream_t st) {

@@ -27,6 +27,7 @@ constexpr int kOffB3 = kOffW3 + kMlpOut * kMlpHidden;
 constexpr int kMlpParams = kOffB3 + kMlpOut;                 // 6426
 constexpr int kRecordFloats = kMlpIn + 3;                    // features, t', psi_i, psi_j
 constexpr float kKappaMax = 50.0f;
+constexpr float kTEdge = 1e-7f;          // the learned move's t' lies in (kTEdge, 1 - kTEdge)
 constexpr float kTwoPi = 6.283185307179586f;
 
 // Features of a pair at one state: log(1+beta sqrt(S)|h|) for both sites,
@@ -194,7 +195,7 @@ __device__ __forceinline__ bool sample_move(MoveStream& g, const ProposalParams&
     const float x = gamma_sample(g, p.a), y = gamma_sample(g, p.b);
     if (x < 0.f || y < 0.f || x + y <= 0.f) return false;
     t = x / (x + y);
-    if (!(t > 1e-7f && t < 1.0f - 1e-7f)) return false;
+    if (!(t > kTEdge && t < 1.0f - kTEdge)) return false;
     float psi[2];
     for (int s = 0; s < 2; s++) {
         const float u = g.uniform();

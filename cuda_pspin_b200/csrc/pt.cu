@@ -56,6 +56,7 @@ __global__ void __launch_bounds__(256) energy_kernel(const EnergyParams P) {
             sp[idx] = b;
             if (l < U.rep_count) P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l] = b;
         }
+        if (P.renorm_only) return;
         __syncthreads();
     }
 

@@ -9,15 +9,17 @@ sweep.  Steps:
 1. plain PT for `train_sweeps` sweeps with fields at both ends of every
    move; accepted moves are recorded (probability record_prob) into a ring;
 2. the network is trained on the GPU (own forward/backward/Adam kernels);
-3. `measure_sweeps` sweeps of plain PT, then of PT with the learned move
-   (exact MH), then of plain PT again, each recording E and the pair
-   overlaps q of the replicas at temperature slot `slot` after every sweep.
-   The two plain phases bracket the learned one, so a drift of <E> (an
-   unequilibrated start) shows as a difference between them.
+3. `measure_sweeps` sweeps per proposal in `blocks` interleaved blocks,
+   plain and learned (exact MH) alternating in ABBA order, each block
+   recording E and the pair overlaps q of the replicas at temperature slot
+   `slot` after every sweep.  A slow drift of the samples (ageing at low T)
+   then enters both proposals alike; <E> is compared through the per-block
+   paired differences learned - plain, whose spread over blocks gives the
+   error.
 
-Reported per phase: tau_int of E, of q and of q^2 (Sokal windowing, chains =
-samples x replicas or samples x pairs), wall time, <E>/N at the slot with its
-tau-corrected error, and independent samples per second.  T = 0.3 is not on
+Reported per proposal: tau_int of E, of q and of q^2 (Sokal windowing,
+chains = blocks x samples x replicas or pairs), wall time, <E>/N at the slot,
+and independent samples per second.  T = 0.3 is not on
 the 24-point grid in [0.2, 1.6]; the nearest slot is 19 (T = 0.28714).
 """
 from __future__ import annotations
@@ -55,28 +57,36 @@ def run_pt(eng: Engine, sweeps: int, chunk: int = 256) -> float:
     return time.perf_counter() - t0
 
 
-def measure(eng: Engine, proposal: int, sweeps: int, slot: int, N: int) -> dict:
+def measure_block(eng: Engine, proposal: int, sweeps: int, slot: int, N: int) -> dict:
+    """One block of PT with `proposal`: series at the slot, wall time, counters."""
     eng.set_proposal(proposal)
     eng.observe_init(slot, sweeps)
     eng.reset_counters()
     seconds = run_pt(eng, sweeps)
     E, q = eng.observe_get()                                   # [n, S, nrep], [n, S, npairs]
     _, acc, prop = eng.get_results()
-    e = E.reshape(E.shape[0], -1).T / N                        # chains x n
-    qq = q.reshape(q.shape[0], -1).T
+    return {"e": E.reshape(E.shape[0], -1).T / N, "q": q.reshape(q.shape[0], -1).T, "seconds": seconds,
+            "acc": int(acc.sum()), "prop": int(prop.sum())}
+
+
+def summarise(blocks: list[dict], name: str) -> dict:
+    """Blocks are independent chains: tau over all of them, rates over the total time."""
+    e = np.concatenate([b["e"] for b in blocks])               # (blocks x chains) x n
+    qq = np.concatenate([b["q"] for b in blocks])
+    seconds = sum(b["seconds"] for b in blocks)
     te, tq, tq2 = T.tau_int(e), T.tau_int(qq), T.tau_int(qq ** 2)
-    half = e.shape[1] // 2
+    sweeps = sum(b["e"].shape[1] for b in blocks)
     return {
-        "proposal": {PROPOSAL_PLAIN: "plain", PROPOSAL_LEARNED: "learned"}[proposal],
-        "sweeps": sweeps, "seconds": seconds, "sweeps_per_s": sweeps / seconds,
-        "acceptance_all_T": float(acc.sum() / max(prop.sum(), 1)),
+        "proposal": name, "blocks": len(blocks), "sweeps": sweeps, "seconds": seconds,
+        "sweeps_per_s": sweeps / seconds,
+        "acceptance_all_T": sum(b["acc"] for b in blocks) / max(sum(b["prop"] for b in blocks), 1),
         "E_per_N": float(e.mean()), "E_per_N_err": float(np.sqrt(2.0 * te.tau * e.var() / e.size)),
-        "E_per_N_halves": [float(e[:, :half].mean()), float(e[:, half:].mean())],
         "tau_E": te.tau, "tau_E_err": te.err, "tau_E_window": te.window,
         "tau_q": tq.tau, "tau_q_err": tq.err, "tau_q2": tq2.tau, "tau_q2_err": tq2.err,
-        "indep_E_per_s": T.independent_samples_per_second(te, seconds),
-        "indep_q_per_s": T.independent_samples_per_second(tq, seconds),
-        "indep_q2_per_s": T.independent_samples_per_second(tq2, seconds),
+        # chains x n / (2 tau) over the wall time of all blocks
+        "indep_E_per_s": e.size / (2.0 * te.tau) / seconds,
+        "indep_q_per_s": qq.size / (2.0 * tq.tau) / seconds,
+        "indep_q2_per_s": qq.size / (2.0 * tq2.tau) / seconds,
         "q2": float((qq ** 2).mean()),
     }
 
@@ -86,7 +96,8 @@ def run(args) -> dict:
     out = {"workload": {"N": args.N, "samples": args.samples, "NT": args.NT, "nrep": args.nrep,
                         "gamma": args.gamma, "Tmin": args.Tmin, "Tmax": args.Tmax, "slot": args.slot,
                         "T_slot": float(temps[args.slot]), "train_sweeps": args.train_sweeps,
-                        "measure_sweeps": args.measure_sweeps, "seed0": args.seed0}}
+                        "measure_sweeps_per_proposal": args.measure_sweeps, "blocks_per_proposal": args.blocks,
+                        "seed0": args.seed0}}
     eng.learn_init(seed=args.net_seed, capacity=args.capacity, record_prob=args.record_prob)
     eng.set_proposal(PROPOSAL_PLAIN_FIELDS)
     t_rec = run_pt(eng, args.train_sweeps)
@@ -106,17 +117,29 @@ def run(args) -> dict:
         eng.set_proposal(PROPOSAL_PLAIN)
         out["training"]["extra_equilibration_sweeps"] = args.equilibrate
         run_pt(eng, args.equilibrate)
-    p1 = measure(eng, PROPOSAL_PLAIN, args.measure_sweeps, args.slot, args.N)
-    l = measure(eng, PROPOSAL_LEARNED, args.measure_sweeps, args.slot, args.N)
-    p2 = measure(eng, PROPOSAL_PLAIN, args.measure_sweeps, args.slot, args.N)
-    out["plain"], out["learned"], out["plain_after"] = p1, l, p2
+    # interleaved blocks in ABBA order: a slow drift of the samples (ageing)
+    # enters both proposals alike
+    per = args.measure_sweeps // args.blocks
+    plain, learned, diffs = [], [], []
+    for b in range(args.blocks):
+        order = (PROPOSAL_PLAIN, PROPOSAL_LEARNED) if b % 2 == 0 else (PROPOSAL_LEARNED, PROPOSAL_PLAIN)
+        got = {}
+        for prop in order:
+            got[prop] = measure_block(eng, prop, per, args.slot, args.N)
+        plain.append(got[PROPOSAL_PLAIN])
+        learned.append(got[PROPOSAL_LEARNED])
+        diffs.append(float(got[PROPOSAL_LEARNED]["e"].mean() - got[PROPOSAL_PLAIN]["e"].mean()))
+    p, l = summarise(plain, "plain"), summarise(learned, "learned")
+    out["plain"], out["learned"] = p, l
     for key in ("E", "q", "q2"):
-        plain_rate = 0.5 * (p1[f"indep_{key}_per_s"] + p2[f"indep_{key}_per_s"])
-        out[f"gain_{key}"] = l[f"indep_{key}_per_s"] / plain_rate
-    ep = 0.5 * (p1["E_per_N"] + p2["E_per_N"])
-    sp = 0.5 * np.hypot(p1["E_per_N_err"], p2["E_per_N_err"])
-    out["E_diff_sigma"] = (l["E_per_N"] - ep) / np.hypot(l["E_per_N_err"], sp)
-    out["plain_drift_sigma"] = (p2["E_per_N"] - p1["E_per_N"]) / np.hypot(p1["E_per_N_err"], p2["E_per_N_err"])
+        out[f"gain_{key}"] = l[f"indep_{key}_per_s"] / p[f"indep_{key}_per_s"]
+    d = np.asarray(diffs)
+    out["E_diff_per_block"] = diffs
+    out["E_diff_mean"] = float(d.mean())
+    out["E_diff_err"] = float(d.std(ddof=1) / np.sqrt(len(d))) if len(d) > 1 else float("nan")
+    out["E_diff_sigma"] = out["E_diff_mean"] / out["E_diff_err"] if len(d) > 1 else float("nan")
+    block_means = [float(b["e"].mean()) for b in plain]
+    out["plain_block_means"] = block_means
     eng.free()
     return out
 
@@ -134,7 +157,8 @@ def main(argv=None) -> int:
     ap.add_argument("--seed0", type=int, default=42)
     ap.add_argument("--train-sweeps", type=int, default=1 << 14)
     ap.add_argument("--equilibrate", type=int, default=0, help="plain PT sweeps between training and measuring")
-    ap.add_argument("--measure-sweeps", type=int, default=1 << 14)
+    ap.add_argument("--measure-sweeps", type=int, default=1 << 14, help="per proposal, over all blocks")
+    ap.add_argument("--blocks", type=int, default=16, help="interleaved blocks per proposal")
     ap.add_argument("--capacity", type=int, default=1 << 22)
     ap.add_argument("--record-prob", type=float, default=0.01)
     ap.add_argument("--train-steps", type=int, default=3000)

@@ -67,6 +67,8 @@ typedef struct pspin_config {
 
 /* Engine options with no reference counterpart.  Zero-initialised means
  * the defaults (reference-compatible init, resync every 1024 sweeps). */
+enum { PSPIN_RESYNC_FP64 = 0, PSPIN_RESYNC_TC = 1 };
+
 typedef struct pspin_options {
     int init_exact;      /* 1: full-sum spin normalisation; 0 (default): the
                             reference's shared-memory tree (spins.cu:27-69),
@@ -80,7 +82,16 @@ typedef struct pspin_options {
     int quiet;           /* suppress the reference's stdout lines */
     int generic_lists;   /* 1: per-entry site lists for every sample; 0 (default):
                             fully connected dense samples use blocked tiles */
-    int reserved[6];
+    int graph_steps;     /* pspin_pt_run replays a CUDA graph of this many PT
+                            steps (sweeps + exchange); 0 -> 32, <0 -> direct
+                            launches.  Results are identical either way. */
+    int resync_method;   /* PSPIN_RESYNC_FP64 (default) or PSPIN_RESYNC_TC:
+                            periodic energies from the split-BF16 tensor-core
+                            contraction (one dense sample per handle) */
+    int cluster_size;    /* CTAs (a thread-block cluster) sharing one replica
+                            block's lists: 1, 2, 4, 8 or 16 with
+                            cluster_size * warps_per_unit <= 32; 0 -> 1 */
+    int reserved[3];
 } pspin_options;
 
 typedef struct pspin_info {
@@ -155,6 +166,14 @@ int  pspin_pt_run(pspin_state* s, int nsweeps);
  * cumulative exchange counters [NT-1] of one sample. */
 int  pspin_pt_get(pspin_state* s, int sample, int32_t* perm, int64_t* ex_acc, int64_t* ex_prop);
 int  pspin_pt_sweeps_done(pspin_state* s, int64_t* sweeps);
+/* Block-shape autotuner (no reference counterpart): times `sweeps` sweeps
+ * for every shape -- clusters of 1, 2, 4, 8, 16 CTAs per replica block x
+ * 1, 2, 4, 8 warps per CTA (clusters only for the plain proposal) -- on
+ * the handle's own samples, restoring amplitudes, energies, counters and the
+ * sweep index after each trial, and keeps the fastest for later sweeps.
+ * ms_per_sweep[5][4] (or NULL) receives the timings, -1 where a shape does
+ * not fit or does not apply. */
+int  pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int* chosen_cluster, float* ms_per_sweep);
 /* Observable series at one temperature slot (no reference counterpart; the
  * reference writes E every save_freq sweeps to energy_accept.txt and
  * configurations to configs.bin, parallel_tempering.cu:355-416).  After
@@ -176,6 +195,9 @@ enum { PSPIN_FIELDS_FP64 = 0,      /* FP64 sum over the quartet table */
  * the fields.  h [nrep][N][re,im], energy [nrep] (may be NULL).  The
  * tensor-core method builds the symmetric pair-space coupling matrix on its
  * first call for the sample (C(N,2)^2 BF16 x 3 on the device). */
+/* |E_running - E_recomputed| per replica (all samples) at the last periodic
+ * resync, before the running energy was overwritten. */
+int  pspin_resync_drift(pspin_state* s, double* drift);
 int  pspin_local_fields(pspin_state* s, int sample, int method, double* h, double* energy);
 
 /* ---- learned pair proposal (no reference counterpart) ----------------- */

@@ -205,9 +205,13 @@ def test_learned_moves_mh_ratio_against_float64(ps, orc):
         ai, aj = complex(*r["ai_old"]), complex(*r["aj_old"])
         ain, ajn = complex(*r["ai_new"]), complex(*r["aj_new"])
         assert s[i] == ai and s[j] == aj
-        # the decision is the recorded comparison
-        assert bool(r["accepted"]) == bool(r["log_u"] < np.float32(-beta * r["dE"]) + r["log_q_ratio"])
-        if ain != ai or ajn != aj:
+        # the decision is the recorded comparison, for a current t inside the
+        # sampler's interval (1e-7, 1 - 1e-7); outside it the move has no reverse
+        a2, b2 = np.float32(abs(ai) ** 2), np.float32(abs(aj) ** 2)
+        t_cur = a2 / (a2 + b2)
+        t_in = 1e-7 < t_cur < 1 - 1e-7
+        assert bool(r["accepted"]) == (t_in and bool(r["log_u"] < np.float32(-beta * r["dE"]) + r["log_q_ratio"]))
+        if (ain != ai or ajn != aj) and t_in:
             x1 = s.copy()
             x1[i], x1[j] = ain, ajn
             hi1, hj1 = site_field(ref, s, i), site_field(ref, s, j)
