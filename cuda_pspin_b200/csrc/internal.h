@@ -107,6 +107,9 @@ struct SweepParams {
 
 // shared memory bytes of one sweep CTA: amplitudes, per-warp field
 // partials, per-warp chunk rings, ring mbarriers
+#ifdef __CUDACC__
+__host__ __device__
+#endif
 inline size_t sweep_smem_bytes(int N, int warps) {
     return (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)warps * kRepBlock * sizeof(float4) +
            (size_t)warps * kStages * kStage * sizeof(int2) + (size_t)warps * kStages * sizeof(uint64_t);

@@ -42,8 +42,14 @@ __device__ __forceinline__ void st_cluster_f4(const void* local, uint32_t rank, 
                  : "memory");
 }
 
+// the exchange buffer follows the plain kernel's layout, rounded up to 16
+// bytes (float4 stores and loads; with one warp that layout ends at 8 mod 16)
+__host__ __device__ inline size_t cluster_buffer_offset(int N, int warps) {
+    return (sweep_smem_bytes(N, warps) + 15) & ~(size_t)15;
+}
+
 inline size_t cluster_smem_bytes(int N, int warps, int C) {
-    return sweep_smem_bytes(N, warps) + (size_t)2 * C * kRepBlock * sizeof(float4);
+    return cluster_buffer_offset(N, warps) + (size_t)2 * C * kRepBlock * sizeof(float4);
 }
 
 template <int VARIANT>
@@ -64,7 +70,7 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     int2* ring = ring_all + (size_t)warp * kStages * kStage;
     uint64_t* bars_all = reinterpret_cast<uint64_t*>(ring_all + (size_t)W * kStages * kStage);
     uint64_t* bars = bars_all + warp * kStages;
-    float4* cred = reinterpret_cast<float4*>(bars_all + W * kStages);         // [2][C][32]
+    float4* cred = reinterpret_cast<float4*>(smem_raw + cluster_buffer_offset(N, W));   // [2][C][32]
 
     const bool active = lane < U.rep_count;
     const bool writer = rank == 0;

@@ -20,6 +20,8 @@ def _cfgs(ps, orc, **kw):
     (0, dict(N=24, nrep=16, fmc_mode=0, seed=3, J0=0.5), 16, 2),
     (0, dict(N=20, nrep=8, fmc_mode=0, seed=9), 8, 4),
     (1, dict(N=16, nrep=8, fmc_mode=1, seed=11), 4, 2),
+    (0, dict(N=12, nrep=8, fmc_mode=0, seed=2), 4, 1),        # one warp: exchange buffer alignment
+    (1, dict(N=16, nrep=8, fmc_mode=1, seed=12), 2, 1),
 ])
 def test_cluster_sweep_dE_against_fp64(ps, orc, variant, kw, cluster, warps):
     c, oc = _cfgs(ps, orc, **kw)
