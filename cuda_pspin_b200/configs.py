@@ -39,58 +39,67 @@ REF_KEYS = {"1": "config1_dense_pt_n32_fmc2", "2": "config2_sparse_pt_n512_comb"
             "5": "config5_dense_pt_n64_fmc2"}
 
 
-def _pt_engine(N, seeds, NT, nrep, variant, fmc, gamma, Tmin=0.2, Tmax=1.6):
+def _pt_engine(N, seeds, NT, nrep, variant, fmc, gamma, shape, Tmin=0.2, Tmax=1.6):
     cfgs = []
     for s in seeds:
         c = default_config(N=N, nrep=NT * nrep, seed=s, fmc_mode=fmc)
         c.gamma = gamma
         cfgs.append(c)
     t0 = time.perf_counter()
-    eng = Engine(cfgs, variant, make_options(quiet=True))
+    eng = Engine(cfgs, variant, _options(shape))
     setup = time.perf_counter() - t0
     _, betas = temperature_schedule(NT, Tmin, Tmax, True)
     eng.pt_init(NT, nrep, betas, 1)
     return eng, setup
 
 
-def _timed(eng, run, sweeps, warmup, tune_sweeps):
+def _options(shape, **kw):
+    w, c = shape if shape else (0, 0)
+    return make_options(quiet=True, warps_per_unit=w, cluster_size=c, **kw)
+
+
+def _timed(eng, run, sweeps, warmup, tune_sweeps, shape):
     run(warmup)
-    w, c, ms = eng.autotune(tune_sweeps)
+    if shape:
+        w, c = shape
+    else:
+        w, c, ms = eng.autotune(tune_sweeps)
     run(warmup)
     t0 = time.perf_counter()
     run(sweeps)
     return time.perf_counter() - t0, w, c
 
 
-def measure(config: str, sweeps: int | None = None) -> dict:
+def measure(config: str, sweeps: int | None = None, shape=None) -> dict:
     if config == "1":
-        eng, setup = _pt_engine(32, [42], 20, 4, PSPIN_DENSE, 2, 0.1)
+        eng, setup = _pt_engine(32, [42], 20, 4, PSPIN_DENSE, 2, 0.1, shape)
         sweeps = sweeps or 4096
         run = eng.pt_run
     elif config == "2":
-        eng, setup = _pt_engine(512, [42], 32, 4, PSPIN_SPARSE, 1, 1.0)
+        eng, setup = _pt_engine(512, [42], 32, 4, PSPIN_SPARSE, 1, 1.0, shape)
         sweeps = sweeps or 4096
         run = eng.pt_run
     elif config == "4":
         c = default_config(N=128, nrep=64, seed=42, fmc_mode=0, T=0.5)
         t0 = time.perf_counter()
-        eng = Engine(c, PSPIN_DENSE, make_options(quiet=True))
+        eng = Engine(c, PSPIN_DENSE, _options(shape))
         setup = time.perf_counter() - t0
         eng.fill_betas(2.0)
         sweeps = sweeps or 64
         run = eng.sweep
     elif config == "5":
-        eng, setup = _pt_engine(64, [42], 24, 4, PSPIN_DENSE, 2, 0.1)
+        eng, setup = _pt_engine(64, [42], 24, 4, PSPIN_DENSE, 2, 0.1, shape)
         sweeps = sweeps or 2048
         run = eng.pt_run
     elif config == "5x64":
-        eng, setup = _pt_engine(64, list(range(42, 106)), 24, 4, PSPIN_DENSE, 2, 0.1)
+        eng, setup = _pt_engine(64, list(range(42, 106)), 24, 4, PSPIN_DENSE, 2, 0.1, shape)
         sweeps = sweeps or 1024
         run = eng.pt_run
     else:
         raise ValueError(config)
     moves = sum(N * R // 2 for N, R in zip(eng.Ns, eng.Rs))
-    secs, w, cl = _timed(eng, run, sweeps, warmup=8, tune_sweeps=2 if config == "4" else 8)
+    secs, w, cl = _timed(eng, run, sweeps, warmup=8 if config != "4" else 2,
+                         tune_sweeps=2 if config == "4" else 8, shape=shape)
     eng.free()
     out = {"config": config, "sweeps": sweeps, "seconds": secs, "pair_moves_per_s": moves * sweeps / secs,
            "warps_per_cta": w, "ctas_per_replica_block": cl, "setup_s": setup}
@@ -133,9 +142,12 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--configs", default="1,2,4,5,5x64")
     ap.add_argument("--precision", action="store_true")
+    ap.add_argument("--sweeps", type=int, default=0, help="timed sweeps (0: the configuration's default)")
+    ap.add_argument("--shape", default="", help="W,C: warps per CTA and CTAs per replica block (skips the autotuner)")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
-    res = [measure(k) for k in a.configs.split(",") if k]
+    shape = tuple(int(x) for x in a.shape.split(",")) if a.shape else None
+    res = [measure(k, a.sweeps or None, shape) for k in a.configs.split(",") if k]
     if a.precision:
         res.append(precision())
     for r in res:
