@@ -122,6 +122,9 @@ def load_library() -> ctypes.CDLL:
         "pspin_observe_init": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
         "pspin_autotune": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp]),
         "pspin_resync_drift": (ctypes.c_int, [vp, vp]),
+        "pspin_checkpoint_save": (ctypes.c_int, [vp, ctypes.c_char_p]),
+        "pspin_pt_shape": (ctypes.c_int, [vp, vp, vp, vp]),
+        "pspin_checkpoint_load": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "pspin_observe_get": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int]),
         "pspin_learn_init": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_float]),
         "pspin_learn_params": (ctypes.c_int, [vp, vp, vp]),
@@ -327,6 +330,17 @@ class Engine:
         _check(self._lib.pspin_pt_get(self._h, sample, _ptr(perm), _ptr(acc), _ptr(prop)))
         return perm, acc, prop
 
+    def checkpoint_save(self, path: str) -> None:
+        _check(self._lib.pspin_checkpoint_save(self._h, os.fsencode(path)))
+
+    def checkpoint_load(self, path: str) -> None:
+        """Restores a checkpoint written by a handle built from the same configurations."""
+        _check(self._lib.pspin_checkpoint_load(self._h, os.fsencode(path)))
+        NT, nr, fq = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        _check(self._lib.pspin_pt_shape(self._h, ctypes.byref(NT), ctypes.byref(nr), ctypes.byref(fq)))
+        if NT.value >= 2:
+            self.NT, self.nrep_per_temp = NT.value, nr.value
+
     def resync_drift(self) -> np.ndarray:
         """|E_running - E_recomputed| per replica at the last periodic resync."""
         d = np.empty(self.n_replicas, np.float64)
@@ -334,9 +348,10 @@ class Engine:
         return d
 
     def autotune(self, sweeps: int = 8):
-        """(warps per CTA, CTAs per replica block, ms per sweep [cluster 1,2,4,8,16][warps 1,2,4,8])."""
+        """(warps per CTA, CTAs per replica block (0: list-resident one-warp kernel),
+        ms per sweep [resident, cluster 1, 2, 4, 8, 16][warps 1, 2, 4, 8])."""
         w, c = ctypes.c_int(0), ctypes.c_int(0)
-        ms = np.zeros((5, 4), np.float32)
+        ms = np.zeros((6, 4), np.float32)
         _check(self._lib.pspin_autotune(self._h, int(sweeps), ctypes.byref(w), ctypes.byref(c), _ptr(ms)))
         return w.value, c.value, ms
 

@@ -54,7 +54,8 @@ def _pt_engine(N, seeds, NT, nrep, variant, fmc, gamma, shape, Tmin=0.2, Tmax=1.
 
 
 def _options(shape, **kw):
-    w, c = shape if shape else (0, 0)
+    w, c = shape if shape else (0, None)
+    c = 0 if c is None else (-1 if c == 0 else c)      # 0 from the autotuner: the list-resident kernel
     return make_options(quiet=True, warps_per_unit=w, cluster_size=c, **kw)
 
 

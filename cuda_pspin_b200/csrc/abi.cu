@@ -140,7 +140,9 @@ struct pspin_state {
     std::vector<SampleHost> hs;
     std::vector<SampleDev> sd;
     std::vector<Unit> units;
-    int R_tot = 0, max_N = 0, warps = 8, cluster = 1;
+    int R_tot = 0, max_N = 0, warps = 8, cluster = 1;   // cluster 0: list-resident one-warp kernel
+    int64_t max_site_entries = 0;
+    int warps2 = 8;                     // warps per CTA of the two-pass (learned / fields) sweep
     int64_t spin_total = 0;
     cudaStream_t st = nullptr;
     int device = 0;
@@ -937,12 +939,21 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     });
     s->warps = choose_warps(s);
     if (s->warps < 0) return bail(fail(PSPIN_ERR_ARG, "warps_per_unit must be 1, 2, 4 or 8"));
+    for (const SampleHost& h : s->hs) s->max_site_entries = std::max<int64_t>(s->max_site_entries, h.site_entries);
     {
         const int c = s->opt.cluster_size == 0 ? 1 : s->opt.cluster_size;
-        if (c != 1 && c != 2 && c != 4 && c != 8 && c != 16)
-            return bail(fail(PSPIN_ERR_ARG, "cluster_size must be 1, 2, 4, 8 or 16"));
-        if (c * s->warps > kSplit) return bail(fail(PSPIN_ERR_ARG, "cluster_size * warps_per_unit must be <= 32"));
-        s->cluster = c;
+        s->warps2 = s->warps;
+        if (c == -1) {
+            if (resident_smem_bytes_host(s->max_N, s->max_site_entries) > 227 * 1024)
+                return bail(fail(PSPIN_ERR_ARG, "the site lists do not fit in shared memory (cluster_size -1)"));
+            s->cluster = 0;
+            s->warps = 1;
+        } else {
+            if (c != 1 && c != 2 && c != 4 && c != 8 && c != 16)
+                return bail(fail(PSPIN_ERR_ARG, "cluster_size must be -1, 1, 2, 4, 8 or 16"));
+            if (c * s->warps > kSplit) return bail(fail(PSPIN_ERR_ARG, "cluster_size * warps_per_unit must be <= 32"));
+            s->cluster = c;
+        }
     }
     if (sweep_smem_bytes(s->max_N, s->warps) > 227 * 1024)
         return bail(fail(PSPIN_ERR_ARG, "N=%d needs more shared memory than a CTA has", s->max_N));
@@ -1041,7 +1052,7 @@ static int enqueue_step(pspin_state* s, int nsweeps, bool exchange, cudaEvent_t 
     p.pair_chunks = s->d_pair_chunks;
     p.sweep_counter = s->d_sweep_counter;
     p.nsweeps = nsweeps;
-    p.warps = s->warps;
+    p.warps = s->proposal == PSPIN_PROPOSAL_PLAIN ? s->warps : s->warps2;
     p.trace_sample = s->opt.trace_sample;
     p.trace_rep = s->opt.trace_replica;
     p.trace_cap = s->opt.trace_capacity;
@@ -1050,7 +1061,9 @@ static int enqueue_step(pspin_state* s, int nsweeps, bool exchange, cudaEvent_t 
     p.status = s->d_status;
     if (e0) CK(cudaEventRecord(e0, s->st));
     p.cluster = s->proposal == PSPIN_PROPOSAL_PLAIN ? s->cluster : 1;
-    if (s->proposal == PSPIN_PROPOSAL_PLAIN && s->cluster > 1) {
+    if (s->proposal == PSPIN_PROPOSAL_PLAIN && s->cluster == 0) {
+        CK(launch_sweep_resident(p, (int)s->units.size(), s->variant, s->max_N, s->max_site_entries, s->st));
+    } else if (s->proposal == PSPIN_PROPOSAL_PLAIN && s->cluster > 1) {
         CK(launch_sweep_cluster(p, (int)s->units.size(), s->variant, s->max_N, s->st, nullptr));
     } else if (s->proposal == PSPIN_PROPOSAL_PLAIN) {
         CK(launch_sweep(p, (int)s->units.size(), s->variant, s->max_N, s->st));
@@ -1216,6 +1229,9 @@ static int run_sweeps(pspin_state* s, int nsweeps, bool pt) {
 // Whether `cluster` CTAs of `warps` warps can hold one replica block (shared
 // memory, co-residency of the cluster); the plain kernel for cluster 1.
 static bool shape_fits(pspin_state* s, int warps, int cluster) {
+    if (cluster == 0)
+        return s->proposal == PSPIN_PROPOSAL_PLAIN && warps == 1 &&
+               resident_smem_bytes_host(s->max_N, s->max_site_entries) <= 227 * 1024;
     if (cluster * warps > kSplit) return false;
     if (s->proposal != PSPIN_PROPOSAL_PLAIN) return cluster == 1 && learned_smem_bytes_host(s->max_N, warps) <= 227 * 1024;
     if (cluster == 1) return sweep_smem_bytes(s->max_N, warps) <= 227 * 1024;
@@ -1259,7 +1275,11 @@ extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int
         }
         return cudaSuccess;
     };
-    const int w0 = s->warps, c0 = s->cluster;
+    const bool plain = s->proposal == PSPIN_PROPOSAL_PLAIN;
+    int& W = plain ? s->warps : s->warps2;   // the current proposal's kernel is tuned
+    int c_two_pass = 1;
+    int& Cl = plain ? s->cluster : c_two_pass;
+    const int w0 = W, c0 = Cl;
     const float prob0 = s->rec_prob;
     s->rec_prob = 0.f;                       // trials record no training moves
     cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -1268,13 +1288,13 @@ extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int
     if (e == cudaSuccess) e = cudaEventCreate(&t1);
     int best_w = w0, best_c = c0;
     float best_ms = 0.f;
-    const int cw[4] = {1, 2, 4, 8}, cc[5] = {1, 2, 4, 8, 16};
-    for (int ci = 0; ci < 5; ci++)
+    const int cw[4] = {1, 2, 4, 8}, cc[6] = {0, 1, 2, 4, 8, 16};
+    for (int ci = 0; ci < 6; ci++)
         for (int wi = 0; wi < 4; wi++) {
             float ms = -1.f;
             if (e == cudaSuccess && rc == PSPIN_OK && shape_fits(s, cw[wi], cc[ci])) {
-                s->warps = cw[wi];
-                s->cluster = cc[ci];
+                W = cw[wi];
+                Cl = cc[ci];
                 rc = enqueue_step(s, 1, false, nullptr, nullptr);          // warm-up sweep
                 if (rc == PSPIN_OK) e = cudaEventRecord(t0, s->st);
                 for (int k = 0; k < sweeps && rc == PSPIN_OK && e == cudaSuccess; k++)
@@ -1298,14 +1318,14 @@ extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int
     cudaFree(b_spins); cudaFree(b_E); cudaFree(b_acc); cudaFree(b_prop); cudaFree(b_cnt);
     s->rec_prob = prob0;
     const bool good = rc == PSPIN_OK && e == cudaSuccess;
-    s->warps = good ? best_w : w0;
-    s->cluster = good ? best_c : c0;
+    W = good ? best_w : w0;
+    Cl = good ? best_c : c0;
     drop_graph(s);
     if (rc != PSPIN_OK) return rc;
     if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
     if (status) return fail(PSPIN_ERR_TIMEOUT, "a bounded wait in the sweep kernel expired (status %d)", status);
-    if (chosen_warps) *chosen_warps = s->warps;
-    if (chosen_cluster) *chosen_cluster = s->cluster;
+    if (chosen_warps) *chosen_warps = W;
+    if (chosen_cluster) *chosen_cluster = Cl;
     return PSPIN_OK;
 }
 
@@ -1543,6 +1563,14 @@ extern "C" int pspin_observe_get(pspin_state* s, int64_t* n_rows, double* energy
         CK(cudaMemcpyAsync(overlap, s->d_obs_q, (size_t)m * s->S * npairs * sizeof(double), cudaMemcpyDeviceToHost,
                            s->st));
     CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_pt_shape(pspin_state* s, int* NT, int* nrep_per_temp, int* pt_freq) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (NT) *NT = s->pt_NT;
+    if (nrep_per_temp) *nrep_per_temp = s->pt_nrep;
+    if (pt_freq) *pt_freq = s->pt_freq;
     return PSPIN_OK;
 }
 
@@ -1958,6 +1986,180 @@ extern "C" int pspin_learn_loss_grad(pspin_state* s, const float* records, int n
         for (float v : l) m += v;
         *loss = m / n;
     }
+    return PSPIN_OK;
+}
+
+// ------------------------------------------------------------------ checkpoint / resume
+// A binary file with everything that continues a chain bit for bit: FP32
+// amplitudes, running energies, counters, betas, the device sweep index
+// (which keys the pair and move streams), the resync phase, the PT state and
+// the learned network with its Adam moments.  Loading checks that the handle
+// was built from the same configurations (variant, N, replicas, seed, FMC).
+static const char kCkMagic[8] = {'P', 'S', 'P', 'I', 'N', 'C', 'K', '1'};
+
+namespace {
+struct CkFile {
+    FILE* f = nullptr;
+    bool ok = true;
+    ~CkFile() { if (f) fclose(f); }
+    void put(const void* p, size_t n) { if (ok && n && fwrite(p, 1, n, f) != n) ok = false; }
+    void get(void* p, size_t n) { if (ok && n && fread(p, 1, n, f) != n) ok = false; }
+    template <class T> void put(const T& v) { put(&v, sizeof(T)); }
+    template <class T> void get(T& v) { get(&v, sizeof(T)); }
+};
+}  // namespace
+
+template <class T>
+static int dev_to_file(pspin_state* s, CkFile& f, const T* d, size_t n) {
+    std::vector<T> h(n);
+    if (n) CK(cudaMemcpyAsync(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    f.put(h.data(), n * sizeof(T));
+    return PSPIN_OK;
+}
+
+template <class T>
+static int file_to_dev(pspin_state* s, CkFile& f, T* d, size_t n) {
+    std::vector<T> h(n);
+    f.get(h.data(), n * sizeof(T));
+    if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
+    if (n) CK(cudaMemcpyAsync(d, h.data(), n * sizeof(T), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_checkpoint_save(pspin_state* s, const char* path) {
+    if (!s || !path) return fail(PSPIN_ERR_ARG, "null argument");
+    CkFile f;
+    f.f = fopen(path, "wb");
+    if (!f.f) return fail(PSPIN_ERR_ARG, "cannot open %s for writing", path);
+    CK(cudaStreamSynchronize(s->st));
+    long long counter = 0;
+    CK(cudaMemcpy(&counter, s->d_sweep_counter, sizeof(counter), cudaMemcpyDeviceToHost));
+    f.put(kCkMagic, sizeof(kCkMagic));
+    f.put((int32_t)s->variant);
+    f.put((int32_t)s->S);
+    f.put((int64_t)s->R_tot);
+    f.put((int64_t)s->spin_total);
+    for (const SampleHost& h : s->hs) {
+        f.put((int32_t)h.N);
+        f.put((int32_t)h.R);
+        f.put((uint64_t)h.cfg.seed);
+        f.put((int32_t)h.cfg.fmc_mode);
+    }
+    f.put((int64_t)s->sweeps_done);
+    f.put((int64_t)s->since_resync);
+    f.put((int64_t)counter);
+    f.put((int32_t)s->proposal);
+    f.put((int32_t)s->warps);          // block shapes: they fix the summation order
+    f.put((int32_t)s->cluster);
+    f.put((int32_t)s->warps2);
+    TRY(dev_to_file(s, f, s->d_spins, (size_t)s->spin_total));
+    TRY(dev_to_file(s, f, s->d_E, (size_t)s->R_tot));
+    TRY(dev_to_file(s, f, s->d_beta, (size_t)s->R_tot));
+    TRY(dev_to_file(s, f, s->d_target, (size_t)s->R_tot));
+    TRY(dev_to_file(s, f, s->d_acc, (size_t)s->R_tot));
+    TRY(dev_to_file(s, f, s->d_prop, (size_t)s->R_tot));
+    f.put((int32_t)s->pt_NT);
+    f.put((int32_t)s->pt_nrep);
+    f.put((int32_t)s->pt_freq);
+    if (s->pt_NT >= 2) {
+        const size_t NT = s->pt_NT, nr = s->pt_nrep, S = s->S;
+        TRY(dev_to_file(s, f, s->d_beta_sched, NT));
+        TRY(dev_to_file(s, f, s->d_perm, S * NT * nr));
+        TRY(dev_to_file(s, f, s->d_drand, S));
+        TRY(dev_to_file(s, f, s->d_ex_acc, S * (NT - 1)));
+        TRY(dev_to_file(s, f, s->d_ex_prop, S * (NT - 1)));
+    }
+    const int32_t has_net = s->d_w32 ? 1 : 0;
+    f.put(has_net);
+    if (has_net) {
+        f.put((int32_t)s->adam_t);
+        f.put((uint64_t)s->learn_seed);
+        f.put((float)s->rec_prob);
+        f.put((int32_t)s->rec_cap);
+        TRY(dev_to_file(s, f, s->d_w32, (size_t)kMlpParamsHost));
+        TRY(dev_to_file(s, f, s->d_adam_m, (size_t)kMlpParamsHost));
+        TRY(dev_to_file(s, f, s->d_adam_v, (size_t)kMlpParamsHost));
+    }
+    if (!f.ok) return fail(PSPIN_ERR_ARG, "write to %s failed", path);
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_checkpoint_load(pspin_state* s, const char* path) {
+    if (!s || !path) return fail(PSPIN_ERR_ARG, "null argument");
+    CkFile f;
+    f.f = fopen(path, "rb");
+    if (!f.f) return fail(PSPIN_ERR_ARG, "cannot open %s", path);
+    char magic[8];
+    f.get(magic, sizeof(magic));
+    if (!f.ok || std::memcmp(magic, kCkMagic, sizeof(magic)) != 0) return fail(PSPIN_ERR_ARG, "%s is not a checkpoint", path);
+    int32_t variant = 0, S = 0;
+    int64_t R_tot = 0, spin_total = 0;
+    f.get(variant); f.get(S); f.get(R_tot); f.get(spin_total);
+    if (!f.ok || variant != s->variant || S != s->S || R_tot != s->R_tot || spin_total != s->spin_total)
+        return fail(PSPIN_ERR_ARG, "checkpoint does not match this handle (variant, samples or replicas)");
+    for (const SampleHost& h : s->hs) {
+        int32_t N = 0, R = 0, fmc = 0;
+        uint64_t seed = 0;
+        f.get(N); f.get(R); f.get(seed); f.get(fmc);
+        if (!f.ok || N != h.N || R != h.R || seed != (uint64_t)h.cfg.seed || fmc != h.cfg.fmc_mode)
+            return fail(PSPIN_ERR_ARG, "checkpoint does not match this handle (a sample's N, replicas, seed or FMC)");
+    }
+    int64_t sweeps_done = 0, since_resync = 0, counter = 0;
+    int32_t proposal = 0, warps = 0, cluster = 0, warps2 = 0;
+    f.get(sweeps_done); f.get(since_resync); f.get(counter); f.get(proposal);
+    f.get(warps); f.get(cluster); f.get(warps2);
+    if (!f.ok || warps < 1 || warps > 8 || warps2 < 1 || warps2 > 8 || cluster < 0 || cluster > 16)
+        return fail(PSPIN_ERR_ARG, "checkpoint file is truncated or corrupt");
+    if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
+    TRY(file_to_dev(s, f, s->d_spins, (size_t)s->spin_total));
+    TRY(file_to_dev(s, f, s->d_E, (size_t)s->R_tot));
+    std::vector<double> betas(s->R_tot);
+    f.get(betas.data(), betas.size() * sizeof(double));
+    TRY(file_to_dev(s, f, s->d_target, (size_t)s->R_tot));
+    TRY(file_to_dev(s, f, s->d_acc, (size_t)s->R_tot));
+    TRY(file_to_dev(s, f, s->d_prop, (size_t)s->R_tot));
+    int32_t NT = 0, nrep = 0, freq = 0;
+    f.get(NT); f.get(nrep); f.get(freq);
+    if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
+    if (NT >= 2) {
+        std::vector<double> sched(NT);
+        f.get(sched.data(), sched.size() * sizeof(double));
+        if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
+        TRY(pspin_pt_init(s, NT, nrep, sched.data(), freq));
+        const size_t SS = s->S;
+        TRY(file_to_dev(s, f, s->d_perm, SS * NT * nrep));
+        TRY(file_to_dev(s, f, s->d_drand, SS));
+        TRY(file_to_dev(s, f, s->d_ex_acc, SS * (NT - 1)));
+        TRY(file_to_dev(s, f, s->d_ex_prop, SS * (NT - 1)));
+    }
+    CK(cudaMemcpyAsync(s->d_beta, betas.data(), betas.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    int32_t has_net = 0;
+    f.get(has_net);
+    if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
+    if (has_net) {
+        int32_t adam_t = 0, cap = 0;
+        uint64_t seed = 0;
+        float prob = 0.f;
+        f.get(adam_t); f.get(seed); f.get(prob); f.get(cap);
+        if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
+        TRY(pspin_learn_init(s, seed, std::max(cap, 1), prob));
+        TRY(file_to_dev(s, f, s->d_w32, (size_t)kMlpParamsHost));
+        TRY(file_to_dev(s, f, s->d_adam_m, (size_t)kMlpParamsHost));
+        TRY(file_to_dev(s, f, s->d_adam_v, (size_t)kMlpParamsHost));
+        CK(launch_to_bf16(s->d_w32, s->d_wbf, s->st));
+        s->adam_t = adam_t;
+    }
+    TRY(pspin_set_proposal(s, proposal));
+    CK(cudaMemcpyAsync(s->d_sweep_counter, &counter, sizeof(counter), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    s->sweeps_done = sweeps_done;
+    s->since_resync = since_resync;
+    s->warps = warps;
+    s->cluster = cluster;
+    s->warps2 = warps2;
+    drop_graph(s);
     return PSPIN_OK;
 }
 

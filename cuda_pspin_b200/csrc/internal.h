@@ -120,6 +120,9 @@ cudaError_t launch_sweep(const SweepParams& p, int n_units, int variant, int max
 cudaError_t launch_sweep_cluster(const SweepParams& p, int n_units, int variant, int max_N, cudaStream_t st,
                                  int* max_clusters);
 size_t cluster_smem_bytes_host(int N, int warps, int C);
+cudaError_t launch_sweep_resident(const SweepParams& p, int n_units, int variant, int max_N, int64_t max_entries,
+                                  cudaStream_t st);
+size_t resident_smem_bytes_host(int N, int64_t entries);
 
 struct EnergyParams {
     const SampleDev* samples;

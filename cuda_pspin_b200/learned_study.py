@@ -117,6 +117,13 @@ def run(args) -> dict:
         eng.set_proposal(PROPOSAL_PLAIN)
         out["training"]["extra_equilibration_sweeps"] = args.equilibrate
         run_pt(eng, args.equilibrate)
+    # each proposal's kernel gets its own block shape from the autotuner
+    shapes = {}
+    for prop, name in ((PROPOSAL_PLAIN, "plain"), (PROPOSAL_LEARNED, "learned")):
+        eng.set_proposal(prop)
+        w, c, _ = eng.autotune(4)
+        shapes[name] = {"warps_per_cta": w, "ctas_per_replica_block": c}
+    out["block_shapes"] = shapes
     # interleaved blocks in ABBA order: a slow drift of the samples (ageing)
     # enters both proposals alike
     per = args.measure_sweeps // args.blocks

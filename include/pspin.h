@@ -90,7 +90,9 @@ typedef struct pspin_options {
                             contraction (one dense sample per handle) */
     int cluster_size;    /* CTAs (a thread-block cluster) sharing one replica
                             block's lists: 1, 2, 4, 8 or 16 with
-                            cluster_size * warps_per_unit <= 32; 0 -> 1 */
+                            cluster_size * warps_per_unit <= 32; 0 -> 1;
+                            -1: one warp per block with the sample's whole
+                            lists resident in shared memory (small lists) */
     int reserved[3];
 } pspin_options;
 
@@ -166,13 +168,16 @@ int  pspin_pt_run(pspin_state* s, int nsweeps);
  * cumulative exchange counters [NT-1] of one sample. */
 int  pspin_pt_get(pspin_state* s, int sample, int32_t* perm, int64_t* ex_acc, int64_t* ex_prop);
 int  pspin_pt_sweeps_done(pspin_state* s, int64_t* sweeps);
+/* NT, replicas per temperature and exchange period set by pspin_pt_init (0s before). */
+int  pspin_pt_shape(pspin_state* s, int* NT, int* nrep_per_temp, int* pt_freq);
 /* Block-shape autotuner (no reference counterpart): times `sweeps` sweeps
- * for every shape -- clusters of 1, 2, 4, 8, 16 CTAs per replica block x
- * 1, 2, 4, 8 warps per CTA (clusters only for the plain proposal) -- on
- * the handle's own samples, restoring amplitudes, energies, counters and the
- * sweep index after each trial, and keeps the fastest for later sweeps.
- * ms_per_sweep[5][4] (or NULL) receives the timings, -1 where a shape does
- * not fit or does not apply. */
+ * for every shape -- the list-resident one-warp kernel (row 0), then
+ * clusters of 1, 2, 4, 8, 16 CTAs per replica block x 1, 2, 4, 8 warps per
+ * CTA (resident and clusters only for the plain proposal) -- on the handle's
+ * own samples, restoring amplitudes, energies, counters and the sweep index
+ * after each trial, and keeps the fastest for the current proposal.
+ * ms_per_sweep[6][4] (or NULL) receives the timings, -1 where a shape does
+ * not fit or does not apply; *chosen_cluster 0 means the resident kernel. */
 int  pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int* chosen_cluster, float* ms_per_sweep);
 /* Observable series at one temperature slot (no reference counterpart; the
  * reference writes E every save_freq sweeps to energy_accept.txt and
@@ -222,6 +227,17 @@ int  pspin_learn_records(pspin_state* s, int64_t* n_recorded, float* out /*[max]
 /* Loss and gradient of the mean -log q_L over n host records (FP32
  * weights): the check of the backward pass. */
 int  pspin_learn_loss_grad(pspin_state* s, const float* records, int n, double* loss, float* grad);
+
+/* ---- checkpoint / resume (no reference counterpart) ------------------ */
+/* Everything that continues the chain bit for bit: FP32 amplitudes, running
+ * energies, counters, betas, the sweep index that keys the pair and move
+ * streams, the resync phase, the PT state (pspin_pt_init's schedule, perm,
+ * drand48 states, exchange counters) and the learned network (weights,
+ * Adam moments; not the record ring) and the block shapes (which fix the
+ * summation order of the fields).  Load into a handle created from the same
+ * configurations; anything else is rejected. */
+int  pspin_checkpoint_save(pspin_state* s, const char* path);
+int  pspin_checkpoint_load(pspin_state* s, const char* path);
 
 /* ---- per-move trace (tests) ------------------------------------------ */
 int  pspin_trace_get(pspin_state* s, pspin_move_record* out, int max_records, int* n_records);

@@ -22,6 +22,9 @@ def _cfgs(ps, orc, **kw):
     (1, dict(N=16, nrep=8, fmc_mode=1, seed=11), 4, 2),
     (0, dict(N=12, nrep=8, fmc_mode=0, seed=2), 4, 1),        # one warp: exchange buffer alignment
     (1, dict(N=16, nrep=8, fmc_mode=1, seed=12), 2, 1),
+    (0, dict(N=12, nrep=33, fmc_mode=2, seed=7), -1, 1),      # list-resident one-warp kernel, groups
+    (0, dict(N=16, nrep=8, fmc_mode=0, seed=5), -1, 1),       #   ... fully connected tiles
+    (1, dict(N=24, nrep=8, fmc_mode=1, seed=13), -1, 1),      #   ... sparse
 ])
 def test_cluster_sweep_dE_against_fp64(ps, orc, variant, kw, cluster, warps):
     c, oc = _cfgs(ps, orc, **kw)
