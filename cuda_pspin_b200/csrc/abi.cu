@@ -43,8 +43,9 @@ struct LearnParams {
     int rec_cap;
     float rec_prob;
 };
-cudaError_t launch_learned_sweep(const SweepParams& p, const LearnParams& l, int n_units, int max_N, cudaStream_t st);
-size_t learned_smem_bytes_host(int N, int warps);
+cudaError_t launch_learned_sweep(const SweepParams& p, const LearnParams& l, int n_units, int max_N, cudaStream_t st,
+                                 int* max_clusters);
+size_t learned_smem_bytes_host(int N, int warps, int C);
 cudaError_t launch_mlp_fwd_bwd(const float* w, const float* records, const int* index, int n, float* save,
                                float* loss, cudaStream_t st);
 cudaError_t launch_mlp_grad(const float* save, int n, float* grad, cudaStream_t st);
@@ -142,7 +143,7 @@ struct pspin_state {
     std::vector<Unit> units;
     int R_tot = 0, max_N = 0, warps = 8, cluster = 1;   // cluster 0: list-resident one-warp kernel
     int64_t max_site_entries = 0;
-    int warps2 = 8;                     // warps per CTA of the two-pass (learned / fields) sweep
+    int warps2 = 8, cluster2 = 1;       // block shape of the two-pass (learned / fields) sweep
     int64_t spin_total = 0;
     cudaStream_t st = nullptr;
     int device = 0;
@@ -953,6 +954,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
                 return bail(fail(PSPIN_ERR_ARG, "cluster_size must be -1, 1, 2, 4, 8 or 16"));
             if (c * s->warps > kSplit) return bail(fail(PSPIN_ERR_ARG, "cluster_size * warps_per_unit must be <= 32"));
             s->cluster = c;
+            s->cluster2 = c;
         }
     }
     if (sweep_smem_bytes(s->max_N, s->warps) > 227 * 1024)
@@ -1060,7 +1062,7 @@ static int enqueue_step(pspin_state* s, int nsweeps, bool exchange, cudaEvent_t 
     p.trace = s->d_trace;
     p.status = s->d_status;
     if (e0) CK(cudaEventRecord(e0, s->st));
-    p.cluster = s->proposal == PSPIN_PROPOSAL_PLAIN ? s->cluster : 1;
+    p.cluster = s->proposal == PSPIN_PROPOSAL_PLAIN ? s->cluster : s->cluster2;
     if (s->proposal == PSPIN_PROPOSAL_PLAIN && s->cluster == 0) {
         CK(launch_sweep_resident(p, (int)s->units.size(), s->variant, s->max_N, s->max_site_entries, s->st));
     } else if (s->proposal == PSPIN_PROPOSAL_PLAIN && s->cluster > 1) {
@@ -1075,7 +1077,7 @@ static int enqueue_step(pspin_state* s, int nsweeps, bool exchange, cudaEvent_t 
         lp.rec_count = s->d_rec_count;
         lp.rec_cap = s->rec_cap;
         lp.rec_prob = s->rec_prob;
-        CK(launch_learned_sweep(p, lp, (int)s->units.size(), s->max_N, s->st));
+        CK(launch_learned_sweep(p, lp, (int)s->units.size(), s->max_N, s->st, nullptr));
     }
     if (e1) CK(cudaEventRecord(e1, s->st));
     ExchangeParams x{};
@@ -1233,7 +1235,20 @@ static bool shape_fits(pspin_state* s, int warps, int cluster) {
         return s->proposal == PSPIN_PROPOSAL_PLAIN && warps == 1 &&
                resident_smem_bytes_host(s->max_N, s->max_site_entries) <= 227 * 1024;
     if (cluster * warps > kSplit) return false;
-    if (s->proposal != PSPIN_PROPOSAL_PLAIN) return cluster == 1 && learned_smem_bytes_host(s->max_N, warps) <= 227 * 1024;
+    if (s->proposal != PSPIN_PROPOSAL_PLAIN) {
+        if (learned_smem_bytes_host(s->max_N, warps, cluster) > 227 * 1024) return false;
+        if (cluster == 1) return true;
+        SweepParams p{};
+        p.warps = warps;
+        p.cluster = cluster;
+        LearnParams lp{};
+        int n = 0;
+        if (launch_learned_sweep(p, lp, (int)s->units.size(), s->max_N, s->st, &n) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return n > 0;
+    }
     if (cluster == 1) return sweep_smem_bytes(s->max_N, warps) <= 227 * 1024;
     if (cluster_smem_bytes_host(s->max_N, warps, cluster) > 227 * 1024) return false;
     SweepParams p{};
@@ -1277,8 +1292,7 @@ extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int
     };
     const bool plain = s->proposal == PSPIN_PROPOSAL_PLAIN;
     int& W = plain ? s->warps : s->warps2;   // the current proposal's kernel is tuned
-    int c_two_pass = 1;
-    int& Cl = plain ? s->cluster : c_two_pass;
+    int& Cl = plain ? s->cluster : s->cluster2;
     const int w0 = W, c0 = Cl;
     const float prob0 = s->rec_prob;
     s->rec_prob = 0.f;                       // trials record no training moves
@@ -2054,6 +2068,7 @@ extern "C" int pspin_checkpoint_save(pspin_state* s, const char* path) {
     f.put((int32_t)s->warps);          // block shapes: they fix the summation order
     f.put((int32_t)s->cluster);
     f.put((int32_t)s->warps2);
+    f.put((int32_t)s->cluster2);
     TRY(dev_to_file(s, f, s->d_spins, (size_t)s->spin_total));
     TRY(dev_to_file(s, f, s->d_E, (size_t)s->R_tot));
     TRY(dev_to_file(s, f, s->d_beta, (size_t)s->R_tot));
@@ -2107,10 +2122,11 @@ extern "C" int pspin_checkpoint_load(pspin_state* s, const char* path) {
             return fail(PSPIN_ERR_ARG, "checkpoint does not match this handle (a sample's N, replicas, seed or FMC)");
     }
     int64_t sweeps_done = 0, since_resync = 0, counter = 0;
-    int32_t proposal = 0, warps = 0, cluster = 0, warps2 = 0;
+    int32_t proposal = 0, warps = 0, cluster = 0, warps2 = 0, cluster2 = 0;
     f.get(sweeps_done); f.get(since_resync); f.get(counter); f.get(proposal);
-    f.get(warps); f.get(cluster); f.get(warps2);
-    if (!f.ok || warps < 1 || warps > 8 || warps2 < 1 || warps2 > 8 || cluster < 0 || cluster > 16)
+    f.get(warps); f.get(cluster); f.get(warps2); f.get(cluster2);
+    if (!f.ok || warps < 1 || warps > 8 || warps2 < 1 || warps2 > 8 || cluster < 0 || cluster > 16 || cluster2 < 1 ||
+        cluster2 > 16)
         return fail(PSPIN_ERR_ARG, "checkpoint file is truncated or corrupt");
     if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
     TRY(file_to_dev(s, f, s->d_spins, (size_t)s->spin_total));
@@ -2159,6 +2175,7 @@ extern "C" int pspin_checkpoint_load(pspin_state* s, const char* path) {
     s->warps = warps;
     s->cluster = cluster;
     s->warps2 = warps2;
+    s->cluster2 = cluster2;
     drop_graph(s);
     return PSPIN_OK;
 }

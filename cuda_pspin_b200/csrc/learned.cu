@@ -73,14 +73,32 @@ __device__ __forceinline__ float argf(float2 a) { return atan2f(a.y, a.x); }
 // feat[8][32] + act1, act2 [64][32] + outs[26][32] floats, then the BF16 weights
 constexpr int kMlpSmemFloats = (kMlpIn + 2 * kMlpHidden + kMlpOut) * 32;
 
-inline size_t learned_smem_bytes(int N, int warps) {
+// cluster variant: the partial-field exchange buffer [2][C][32] float4 after
+// the weights, at a 16-byte boundary
+__host__ __device__ inline size_t learned_cluster_buffer_offset(int N, int warps) {
+    return (sweep_smem_bytes(N, warps) + (size_t)kMlpSmemFloats * sizeof(float) +
+            (size_t)kMlpParams * sizeof(__nv_bfloat16) + 15) & ~(size_t)15;
+}
+
+inline size_t learned_smem_bytes(int N, int warps, int C = 1) {
+    if (C > 1) return learned_cluster_buffer_offset(N, warps) + (size_t)2 * C * kRepBlock * sizeof(float4);
     return sweep_smem_bytes(N, warps) + (size_t)kMlpSmemFloats * sizeof(float) +
            (size_t)kMlpParams * sizeof(__nv_bfloat16) + 16;
 }
 
+// CL: one replica block over a thread-block cluster of P.cluster CTAs.  Each
+// CTA reads 1/C of every list; the partial fields of both passes meet in every
+// CTA's exchange buffer (distributed shared memory, one cluster barrier per
+// exchange, double-buffered by exchange parity); every CTA then evaluates the
+// network and takes the same decision on the same numbers, so the amplitude
+// copies stay identical; rank 0 writes records, trace and results.
+template <bool CL>
 __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams P, const LearnParams L) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Unit U = P.units[blockIdx.x];
+    const int C = CL ? P.cluster : 1;
+    const uint32_t rank = CL ? cluster_rank() : 0u;
+    const bool writer = rank == 0;
+    const Unit U = P.units[blockIdx.x / C];
     const SampleDev S = P.samples[U.sample];
     const int N = S.N, R = S.R;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = P.warps;
@@ -96,6 +114,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
     float* act2 = act1 + kMlpHidden * 32;
     float* outs = act2 + kMlpHidden * 32;
     __nv_bfloat16* wsm = reinterpret_cast<__nv_bfloat16*>(outs + kMlpOut * 32);
+    float4* cred = CL ? reinterpret_cast<float4*>(smem_raw + learned_cluster_buffer_offset(N, W)) : nullptr;
 
     const bool active = lane < U.rep_count;
     const int64_t gr = S.rep_off + U.rep_begin + lane;
@@ -132,8 +151,9 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
     st.sweep0 = sweep0;
     st.steps = steps;
     st.total = total;
-    st.part0 = warp * (kSplit / W);
-    st.part1 = (warp + 1) * (kSplit / W);
+    const int TW = C * W, gw = (int)rank * W + warp;
+    st.part0 = gw * (kSplit / TW);
+    st.part1 = (gw + 1) * (kSplit / TW);
     if (lane == 0) {
         for (int s = 0; s < kStages; s++) mbar_init(bars + s, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -157,6 +177,8 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
     };
     for (int s = 0; s < kStages; s++) issue();
     __syncthreads();
+    if (CL) cluster_sync();                    // every CTA runs before the first remote store
+    uint32_t xchg = 0;                         // exchanges so far (buffer parity)
 
     // one pass over this warp's share of two lists: the sites' lists (base 0)
     // or the pair's sub-lists (base 2, always in the group format)
@@ -178,7 +200,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
             }
         }
     };
-    // partial sums of all warps -> warp 0 (one barrier)
+    // partial sums of all warps (and all CTAs of the cluster) -> warp 0
     auto reduce = [&](const float* h) {
         red[warp * kRepBlock + lane] = make_float4(h[0], h[1], h[2], h[3]);
         __syncthreads();
@@ -188,6 +210,20 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
                 const float4 v = red[w * kRepBlock + lane];
                 hs.x += v.x; hs.y += v.y; hs.z += v.z; hs.w += v.w;
             }
+        if (CL) {
+            float4* buf = cred + (size_t)(xchg & 1u) * C * kRepBlock;
+            if (warp == 0)
+                for (int q = 0; q < C; q++) st_cluster_f4(buf + rank * kRepBlock + lane, (uint32_t)q, hs);
+            cluster_sync();
+            if (warp == 0) {
+                hs = buf[lane];
+                for (int q = 1; q < C; q++) {
+                    const float4 v = buf[q * kRepBlock + lane];
+                    hs.x += v.x; hs.y += v.y; hs.z += v.z; hs.w += v.w;
+                }
+            }
+            xchg++;
+        }
         return hs;
     };
 
@@ -313,7 +349,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
                 nacc++;
             }
             nprop++;
-            if (!learned && accept && active && L.records != nullptr && u01f(g.next()) < L.rec_prob) {
+            if (!learned && accept && active && writer && L.records != nullptr && u01f(g.next()) < L.rec_prob) {
                 float f[kMlpIn];
                 pair_features(ai, aj, hi1, hj1, beta, f);
                 const unsigned long long slot = atomicAdd(L.rec_count, 1ull) % (unsigned long long)L.rec_cap;
@@ -324,7 +360,8 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
                 rec[kMlpIn + 1] = psi_i;
                 rec[kMlpIn + 2] = psi_j;
             }
-            if (P.trace != nullptr && U.sample == P.trace_sample && U.rep_begin + lane == P.trace_rep && active) {
+            if (writer && P.trace != nullptr && U.sample == P.trace_sample && U.rep_begin + lane == P.trace_rep &&
+                active) {
                 const long long idx = (sw - P.trace_sweep0) * steps + k;
                 if (idx >= 0 && idx < P.trace_cap) {
                     pspin_move_record* r = reinterpret_cast<pspin_move_record*>(P.trace) + idx;
@@ -342,27 +379,57 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
     }
     if (!ok_wait && lane == 0)
         for (uint32_t q = consumed; q < issued; q++) mbar_wait(bars + q % kStages, (q / kStages) & 1u, P.status);
-    for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
-        const int site = idx >> 5, l = idx & 31;
-        if (l < U.rep_count) P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l] = sp[idx];
+    if (writer) {
+        for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
+            const int site = idx >> 5, l = idx & 31;
+            if (l < U.rep_count) P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l] = sp[idx];
+        }
+        if (warp == 0 && active) {
+            P.energy[gr] = E;
+            P.accepted[gr] += nacc;
+            P.proposed[gr] += nprop;
+        }
     }
-    if (warp == 0 && active) {
-        P.energy[gr] = E;
-        P.accepted[gr] += nacc;
-        P.proposed[gr] += nprop;
-    }
+    if (CL) cluster_sync();                    // no CTA leaves while a remote store may target it
 }
 
-size_t learned_smem_bytes_host(int N, int warps) { return learned_smem_bytes(N, warps); }
+size_t learned_smem_bytes_host(int N, int warps, int C) { return learned_smem_bytes(N, warps, C); }
 
+// max_clusters != null (clusters only): reports how many clusters of this
+// shape can be resident instead of launching (0: the shape does not fit)
 cudaError_t launch_learned_sweep(const SweepParams& p, const LearnParams& l, int n_units, int max_N,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, int* max_clusters) {
     if (n_units <= 0) return cudaSuccess;
-    if (p.pair_chunks == nullptr) return cudaErrorInvalidValue;
-    const size_t smem = learned_smem_bytes(max_N, p.warps);
-    cudaError_t e = cudaFuncSetAttribute(learned_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (p.pair_chunks == nullptr && max_clusters == nullptr) return cudaErrorInvalidValue;
+    const int C = p.cluster > 1 ? p.cluster : 1;
+    if (C > 16 || (kSplit % (C * p.warps)) != 0) return cudaErrorInvalidValue;
+    const size_t smem = learned_smem_bytes(max_N, p.warps, C);
+    if (C == 1) {
+        cudaError_t e = cudaFuncSetAttribute(learned_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        learned_sweep_kernel<false><<<n_units, 32 * p.warps, smem, st>>>(p, l);
+        return cudaGetLastError();
+    }
+    auto kern = learned_sweep_kernel<true>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && C > 8) e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
-    learned_sweep_kernel<<<n_units, 32 * p.warps, smem, st>>>(p, l);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(n_units * C));
+    cfg.blockDim = dim3((unsigned)(32 * p.warps));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (max_clusters) return cudaOccupancyMaxActiveClusters(max_clusters, kern, &cfg);
+    e = cudaLaunchKernelEx(&cfg, kern, p, l);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

@@ -22,26 +22,6 @@
 
 namespace pspin {
 
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-
-__device__ __forceinline__ void cluster_sync() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
-// store v into the same shared-memory location of CTA `rank` of the cluster
-__device__ __forceinline__ void st_cluster_f4(const void* local, uint32_t rank, float4 v) {
-    const uint32_t la = (uint32_t)__cvta_generic_to_shared(local);
-    uint32_t ra;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(la), "r"(rank));
-    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(ra), "f"(v.x), "f"(v.y), "f"(v.z),
-                 "f"(v.w)
-                 : "memory");
-}
-
 // the exchange buffer follows the plain kernel's layout, rounded up to 16
 // bytes (float4 stores and loads; with one warp that layout ends at 8 mod 16)
 __host__ __device__ inline size_t cluster_buffer_offset(int N, int warps) {

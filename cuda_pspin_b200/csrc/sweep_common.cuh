@@ -209,4 +209,27 @@ __device__ __forceinline__ void accumulate_tiles(const int2* __restrict__ R2, in
     }
 }
 
+// ---------------------------------------------------------------- clusters
+// Partial fields of the CTAs of a thread-block cluster meet in every CTA's
+// exchange buffer (distributed shared memory).
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// store v into the same shared-memory location of CTA `rank` of the cluster
+__device__ __forceinline__ void st_cluster_f4(const void* local, uint32_t rank, float4 v) {
+    const uint32_t la = (uint32_t)__cvta_generic_to_shared(local);
+    uint32_t ra;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(la), "r"(rank));
+    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(ra), "f"(v.x), "f"(v.y), "f"(v.z),
+                 "f"(v.w)
+                 : "memory");
+}
+
 }  // namespace pspin

@@ -92,7 +92,9 @@ typedef struct pspin_options {
                             block's lists: 1, 2, 4, 8 or 16 with
                             cluster_size * warps_per_unit <= 32; 0 -> 1;
                             -1: one warp per block with the sample's whole
-                            lists resident in shared memory (small lists) */
+                            lists resident in shared memory (small lists;
+                            plain move only).  Both the plain and the
+                            two-pass sweep start with this shape. */
     int reserved[3];
 } pspin_options;
 
@@ -173,7 +175,7 @@ int  pspin_pt_shape(pspin_state* s, int* NT, int* nrep_per_temp, int* pt_freq);
 /* Block-shape autotuner (no reference counterpart): times `sweeps` sweeps
  * for every shape -- the list-resident one-warp kernel (row 0), then
  * clusters of 1, 2, 4, 8, 16 CTAs per replica block x 1, 2, 4, 8 warps per
- * CTA (resident and clusters only for the plain proposal) -- on the handle's
+ * CTA (the resident kernel only for the plain proposal) -- on the handle's
  * own samples, restoring amplitudes, energies, counters and the sweep index
  * after each trial, and keeps the fastest for the current proposal.
  * ms_per_sweep[6][4] (or NULL) receives the timings, -1 where a shape does

@@ -157,8 +157,11 @@ def test_learned_chain_keeps_plain_stationary_law_at_beta0(ps):
 
 
 @pytest.mark.parametrize("proposal", [1, 2])
-@pytest.mark.parametrize("kw", [dict(N=12, nrep=4, fmc_mode=2, seed=7), dict(N=16, nrep=8, fmc_mode=0, seed=5)])
-def test_two_pass_moves_dE_against_fp64(ps, orc, kw, proposal):
+@pytest.mark.parametrize("kw,shape", [(dict(N=12, nrep=4, fmc_mode=2, seed=7), (0, 0)),
+                                      (dict(N=16, nrep=8, fmc_mode=0, seed=5), (0, 0)),
+                                      (dict(N=16, nrep=8, fmc_mode=0, seed=5), (2, 4)),     # cluster of 4 CTAs
+                                      (dict(N=14, nrep=40, fmc_mode=2, seed=8), (1, 8))])   # cluster of 8, 1 warp
+def test_two_pass_moves_dE_against_fp64(ps, orc, kw, shape, proposal):
     """PLAIN_FIELDS and LEARNED moves evaluate dE from two field passes."""
     c = ps.default_config(**kw)
     if c.fmc_mode > 0 and c.gamma <= 0.0:
@@ -166,7 +169,8 @@ def test_two_pass_moves_dE_against_fp64(ps, orc, kw, proposal):
     ref = orc.DenseInit(orc.cfg(**kw))
     N, rep, nsw = c.N, 1, 10
     cap = nsw * (N // 2)
-    with ps.Engine(c, ps.PSPIN_DENSE, ps.make_options(trace=(0, rep, cap), resync_every=-1)) as eng:
+    opts = ps.make_options(trace=(0, rep, cap), resync_every=-1, warps_per_unit=shape[0], cluster_size=shape[1])
+    with ps.Engine(c, ps.PSPIN_DENSE, opts) as eng:
         eng.learn_init(seed=3, capacity=16)
         eng.set_proposal(proposal)
         s0 = eng.get_spins()[0][rep].copy()
@@ -180,7 +184,8 @@ def test_two_pass_moves_dE_against_fp64(ps, orc, kw, proposal):
     assert 0 < acc[rep] <= prop[rep]
 
 
-def test_learned_moves_mh_ratio_against_float64(ps, orc):
+@pytest.mark.parametrize("shape", [(0, 0), (2, 4)])
+def test_learned_moves_mh_ratio_against_float64(ps, orc, shape):
     kw = dict(N=12, nrep=4, fmc_mode=2, seed=7)
     c = ps.default_config(**kw)
     c.gamma = 1.0 / (2.0 * (c.N - 1))
@@ -188,7 +193,8 @@ def test_learned_moves_mh_ratio_against_float64(ps, orc):
     T, rep, nsw = 0.7, 2, 8
     cap = nsw * (c.N // 2)
     rng = np.random.default_rng(4)
-    with ps.Engine(c, ps.PSPIN_DENSE, ps.make_options(trace=(0, rep, cap), resync_every=-1)) as eng:
+    opts = ps.make_options(trace=(0, rep, cap), resync_every=-1, warps_per_unit=shape[0], cluster_size=shape[1])
+    with ps.Engine(c, ps.PSPIN_DENSE, opts) as eng:
         eng.learn_init(seed=8, capacity=16)
         w = eng.learn_params()
         w = eng.learn_params(w + rng.normal(0, 0.1, w.shape).astype(np.float32))
