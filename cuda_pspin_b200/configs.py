@@ -139,10 +139,32 @@ def precision(sweeps: int = 1 << 12, every: int = 256) -> dict:
             "final_running_vs_fp64_max_abs_per_site": float(np.max(np.abs(E_run - E64)) / c.N)}
 
 
+def fields(repeats: int = 5) -> dict:
+    """All-site local fields of configuration 4 (N=128 FC, 64 replicas): the
+    split-BF16 tcgen05 contraction against the FP64 table sum, time and error."""
+    from . import FIELDS_FP64
+    c = default_config(N=128, nrep=64, seed=42, fmc_mode=0, T=0.5)
+    eng = Engine(c, PSPIN_DENSE, make_options(quiet=True))
+    eng.local_fields(0, FIELDS_TC_BF16X3)                      # operand preparation (once per sample)
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        h_tc, e_tc = eng.local_fields(0, FIELDS_TC_BF16X3)
+    t_tc = (time.perf_counter() - t0) / repeats
+    t0 = time.perf_counter()
+    h64, e64 = eng.local_fields(0, FIELDS_FP64)
+    t_64 = time.perf_counter() - t0
+    eng.free()
+    rel = float(np.abs(h_tc - h64).max() / np.abs(h64).max())
+    return {"config": "4-fields", "N": 128, "replicas": 64, "tc_ms_per_call": t_tc * 1e3, "fp64_ms_per_call": t_64 * 1e3,
+            "fields_max_err_rel_to_max": rel,
+            "energy_max_rel_err": float(np.max(np.abs(e_tc - e64) / np.abs(e64)))}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--configs", default="1,2,4,5,5x64")
     ap.add_argument("--precision", action="store_true")
+    ap.add_argument("--fields", action="store_true", help="tensor-core vs FP64 all-site fields at configuration 4")
     ap.add_argument("--sweeps", type=int, default=0, help="timed sweeps (0: the configuration's default)")
     ap.add_argument("--shape", default="", help="W,C: warps per CTA and CTAs per replica block (skips the autotuner)")
     ap.add_argument("--out", default="")
@@ -151,6 +173,8 @@ def main(argv=None) -> int:
     res = [measure(k, a.sweeps or None, shape) for k in a.configs.split(",") if k]
     if a.precision:
         res.append(precision())
+    if a.fields:
+        res.append(fields())
     for r in res:
         print(json.dumps(r))
     if a.out:

@@ -39,19 +39,27 @@ struct Rec {
 };
 
 // Cuts one site's records (groups or tiles, [begin, end) in int2 units of
-// `site`) into 32 parts of nearly equal size and packs every part in TMA
-// chunks of whole records, <= kStage entries, padded to an even length.
+// `site`) into kSplit/stride pieces of nearly equal size, piece q in part
+// q*stride (the other parts empty), and packs every part in TMA chunks of
+// whole records, <= kStage entries, padded to an even length.  stride 1 for
+// site lists; short lists use a larger stride so that a warp fetches one
+// chunk rather than several tiny ones (a warp owns kSplit/W consecutive
+// parts for any W dividing kSplit).
 static void pack_site(const std::vector<int2>& site, const std::vector<std::pair<int64_t, int64_t>>& groups, int m,
-                      SiteLists& out) {
+                      SiteLists& out, int stride = 1) {
     const int64_t total = (int64_t)site.size();
-    std::vector<size_t> part_first(kSplit + 1, groups.size());
-    part_first[0] = 0;
+    const int pieces = kSplit / stride;
+    std::vector<size_t> bound(pieces + 1, groups.size());
+    bound[0] = 0;
     size_t g = 0;
-    for (int part = 1; part < kSplit; part++) {
-        const int64_t target = (total * part) / kSplit;
+    for (int q = 1; q < pieces; q++) {
+        const int64_t target = (total * q) / pieces;
         while (g < groups.size() && groups[g].first < target) g++;
-        part_first[part] = g;
+        bound[q] = g;
     }
+    std::vector<size_t> part_first(kSplit + 1, groups.size());
+    for (int part = 0; part < kSplit; part++)
+        part_first[part] = (part % stride == 0) ? bound[part / stride] : bound[part / stride + 1];
     int* sc = &out.site_chunks[(size_t)m * (kSplit + 1)];
     for (int part = 0; part < kSplit; part++) {
         sc[part] = (int)out.chunk_start.size();
@@ -76,7 +84,7 @@ static void pack_site(const std::vector<int2>& site, const std::vector<std::pair
 // Sorts one list's records by (p, o1, o2), cuts groups of equal (p, o1) at
 // kGroupMax data entries and packs them as list `id`.
 static void group_and_pack(std::vector<Rec>& v, int id, std::vector<int2>& site,
-                           std::vector<std::pair<int64_t, int64_t>>& groups, SiteLists& out) {
+                           std::vector<std::pair<int64_t, int64_t>>& groups, SiteLists& out, int stride = 1) {
     std::sort(v.begin(), v.end(), [](const Rec& a, const Rec& b) {
         return a.key != b.key ? a.key < b.key : a.o2 < b.o2;
     });
@@ -96,7 +104,7 @@ static void group_and_pack(std::vector<Rec>& v, int id, std::vector<int2>& site,
         groups.push_back({gb, (int64_t)site.size()});
         t = e;
     }
-    pack_site(site, groups, id, out);
+    pack_site(site, groups, id, out, stride);
 }
 
 void build_pair_lists(int N, const double* g2re, int h2_active, const std::vector<QuartetRec>& qs,
@@ -131,7 +139,7 @@ void build_pair_lists(int N, const double* g2re, int h2_active, const std::vecto
     std::vector<std::pair<int64_t, int64_t>> groups;
     std::vector<int2> site;
     for (int id = 0; id < 2 * npairs; id++) {
-        group_and_pack(per[id], id, site, groups, out);
+        group_and_pack(per[id], id, site, groups, out, 4);      // 8 pieces: one chunk per warp at 8 warps
         std::vector<Rec>().swap(per[id]);
     }
 }

@@ -28,43 +28,89 @@ struct LearnParams {
     float rec_prob;
 };
 
-// Network evaluation for the CTA's 32 replicas by all its warps: features
-// feat[8][32] -> act1[64][32] -> act2[64][32] -> outs[26][32], shared memory,
-// lane-contiguous; BF16 weights in shared memory (broadcast reads), FP32
-// accumulation.  Warp w computes units w, w+W, ...; a barrier after each
-// layer (called by every thread of the CTA).
+// Network evaluation for the CTA's 32 replicas by all its warps, on the
+// tensor cores with warp-level mma.sync m16n8k16 (BF16 operands, FP32
+// accumulation): each layer is Out[32 x units] = In[32 x K] W^T, two m16
+// tiles of replicas x n8 tiles of units, the n8 tiles spread over the warps.
+// A fragments come from the activations in shared memory (layout
+// X[k][32], rounded to BF16), B fragments straight from the BF16 weight rows
+// (two consecutive inputs of one unit are one 32-bit word), bias and tanh in
+// the FP32 epilogue.  K is padded to 16 (first layer) and the 26 outputs to
+// 32 with zeros.  (32 x 64 tiles are below tcgen05's smallest M of 64, and
+// the step is latency-bound.)  Fragment layouts: PTX ISA, "Matrix Fragments
+// for mma.m16n8k16 with floating point type".
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                               uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// One layer: X [K][32] floats in shared memory -> Y [units][32];
+// weights w[u*K + k] (BF16), bias bias[u]; act: tanh
+template <int K, int UNITS, bool ACT>
+__device__ __forceinline__ void mlp_layer_mma(const __nv_bfloat16* __restrict__ w, const __nv_bfloat16* __restrict__ bias,
+                                              const float* X, float* Y, int warp, int W, int lane) {
+    constexpr int KP = K < 16 ? 16 : K;          // padded K
+    constexpr int NT = (UNITS + 7) / 8;          // n8 tiles
+    const int g = lane >> 2, t = lane & 3;
+    for (int nt = warp; nt < NT; nt += W) {
+        const int u = nt * 8 + g;                // this lane's unit for the B fragment
+        float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+        for (int k0 = 0; k0 < KP; k0 += 16) {
+            const int ka = k0 + 2 * t, kb = k0 + 2 * t + 8;
+            uint32_t b0 = 0u, b1 = 0u;
+            if (u < UNITS) {
+                if (ka < K) b0 = *reinterpret_cast<const uint32_t*>(w + u * K + ka);
+                if (kb < K) b1 = *reinterpret_cast<const uint32_t*>(w + u * K + kb);
+            }
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++) {
+                const int r = mt * 16 + g;
+                const float x00 = ka < K ? X[ka * 32 + r] : 0.f, x01 = ka < K ? X[(ka + 1) * 32 + r] : 0.f;
+                const float x10 = ka < K ? X[ka * 32 + r + 8] : 0.f, x11 = ka < K ? X[(ka + 1) * 32 + r + 8] : 0.f;
+                const float x20 = kb < K ? X[kb * 32 + r] : 0.f, x21 = kb < K ? X[(kb + 1) * 32 + r] : 0.f;
+                const float x30 = kb < K ? X[kb * 32 + r + 8] : 0.f, x31 = kb < K ? X[(kb + 1) * 32 + r + 8] : 0.f;
+                mma_bf16_16816(acc[mt], pack_bf16x2(x00, x01), pack_bf16x2(x10, x11), pack_bf16x2(x20, x21),
+                               pack_bf16x2(x30, x31), b0, b1);
+            }
+        }
+        // epilogue: D element (row g (+8), col 2t (+1)) -> unit nt*8 + 2t (+1), replica mt*16 + g (+8)
+        const int u0 = nt * 8 + 2 * t;
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            const int uu = u0 + c;
+            if (uu < UNITS) {
+                const float bb = __bfloat162float(bias[uu]);
+#pragma unroll
+                for (int mt = 0; mt < 2; mt++) {
+                    float z0 = acc[mt][c] + bb, z1 = acc[mt][2 + c] + bb;
+                    if (ACT) { z0 = tanhf(z0); z1 = tanhf(z1); }
+                    Y[uu * 32 + mt * 16 + g] = z0;
+                    Y[uu * 32 + mt * 16 + g + 8] = z1;
+                }
+            }
+        }
+    }
+}
+
+// features feat[8][32] -> act1[64][32] -> act2[64][32] -> outs[26][32]; a
+// barrier after each layer (called by every thread of the CTA)
 __device__ __forceinline__ void mlp_block(const __nv_bfloat16* __restrict__ w, const float* feat, float* act1,
                                           float* act2, float* outs, int warp, int W, int lane) {
-    for (int u = warp; u < kMlpHidden; u += W) {
-        float z = __bfloat162float(w[kOffB1 + u]);
-#pragma unroll
-        for (int i = 0; i < kMlpIn; i++) z = fmaf(__bfloat162float(w[kOffW1 + u * kMlpIn + i]), feat[i * 32 + lane], z);
-        act1[u * 32 + lane] = tanhf(z);
-    }
+    mlp_layer_mma<kMlpIn, kMlpHidden, true>(w + kOffW1, w + kOffB1, feat, act1, warp, W, lane);
     __syncthreads();
-    for (int u = warp; u < kMlpHidden; u += W) {
-        float z = __bfloat162float(w[kOffB2 + u]);
-        const __nv_bfloat162* row = reinterpret_cast<const __nv_bfloat162*>(w + kOffW2 + u * kMlpHidden);
-#pragma unroll 8
-        for (int i = 0; i < kMlpHidden / 2; i++) {
-            const float2 wv = __bfloat1622float2(row[i]);
-            z = fmaf(wv.x, act1[(2 * i) * 32 + lane], z);
-            z = fmaf(wv.y, act1[(2 * i + 1) * 32 + lane], z);
-        }
-        act2[u * 32 + lane] = tanhf(z);
-    }
+    mlp_layer_mma<kMlpHidden, kMlpHidden, true>(w + kOffW2, w + kOffB2, act1, act2, warp, W, lane);
     __syncthreads();
-    for (int u = warp; u < kMlpOut; u += W) {
-        float z = __bfloat162float(w[kOffB3 + u]);
-        const __nv_bfloat162* row = reinterpret_cast<const __nv_bfloat162*>(w + kOffW3 + u * kMlpHidden);
-#pragma unroll 8
-        for (int i = 0; i < kMlpHidden / 2; i++) {
-            const float2 wv = __bfloat1622float2(row[i]);
-            z = fmaf(wv.x, act2[(2 * i) * 32 + lane], z);
-            z = fmaf(wv.y, act2[(2 * i + 1) * 32 + lane], z);
-        }
-        outs[u * 32 + lane] = z;
-    }
+    mlp_layer_mma<kMlpHidden, kMlpOut, false>(w + kOffW3, w + kOffB3, act2, outs, warp, W, lane);
     __syncthreads();
 }
 

@@ -85,12 +85,16 @@ struct ProposalParams {
 __device__ __forceinline__ void decode_outputs(const float* o, ProposalParams& p) {
     p.a = 0.05f + softplusf(o[0]);
     p.b = 0.05f + softplusf(o[1]);
+    #pragma unroll
     for (int s = 0; s < 2; s++) {
         const float* q = o + 2 + 12 * s;
         float m = q[0];
+        #pragma unroll
         for (int k = 1; k < 4; k++) m = fmaxf(m, q[k]);
         float z = 0.f;
+        #pragma unroll
         for (int k = 0; k < 4; k++) { p.w[s][k] = expf(q[k] - m); z += p.w[s][k]; }
+        #pragma unroll
         for (int k = 0; k < 4; k++) {
             p.w[s][k] /= z;
             p.mu[s][k] = q[4 + k];
@@ -114,11 +118,13 @@ __device__ __forceinline__ float log_plain_density(float t) {
 
 __device__ __forceinline__ float log_vm_mix(const ProposalParams& p, int s, float psi) {
     float m = -1e30f, v[4];
+    #pragma unroll
     for (int k = 0; k < 4; k++) {
         v[k] = logf(p.w[s][k]) + p.kappa[s][k] * cosf(psi - p.mu[s][k]) - 1.8378770664093453f - log_i0f(p.kappa[s][k]);
         m = fmaxf(m, v[k]);
     }
     float z = 0.f;
+    #pragma unroll
     for (int k = 0; k < 4; k++) z += expf(v[k] - m);
     return m + logf(z);
 }
@@ -197,14 +203,22 @@ __device__ __forceinline__ bool sample_move(MoveStream& g, const ProposalParams&
     t = x / (x + y);
     if (!(t > kTEdge && t < 1.0f - kTEdge)) return false;
     float psi[2];
+#pragma unroll
     for (int s = 0; s < 2; s++) {
+        // component choice by an unrolled scan (constant indices keep the
+        // parameters in registers)
         const float u = g.uniform();
-        int k = 0;
-        float acc = p.w[s][0];
-        while (k < 3 && u > acc) { k++; acc += p.w[s][k]; }
-        const float v = vonmises_sample(g, p.kappa[s][k]);
+        float acc = p.w[s][0], kap = p.kappa[s][0], mu = p.mu[s][0];
+        bool done = u <= acc;
+#pragma unroll
+        for (int k = 1; k < 4; k++) {
+            if (!done) { kap = p.kappa[s][k]; mu = p.mu[s][k]; }
+            acc += p.w[s][k];
+            done = done || u <= acc;
+        }
+        const float v = vonmises_sample(g, kap);
         if (v < -9.0f) return false;
-        psi[s] = p.mu[s][k] + v;
+        psi[s] = mu + v;
     }
     psi_i = psi[0];
     psi_j = psi[1];
@@ -230,16 +244,20 @@ __device__ __forceinline__ float loss_output_grad(const float* o, float t, float
     g[0] = -(logf(t) - digammaf_series(p.a) + dab) * sigmoidf(o[0]);
     g[1] = -(log1pf(-t) - digammaf_series(p.b) + dab) * sigmoidf(o[1]);
     const float psis[2] = {psi_i, psi_j};
+    #pragma unroll
     for (int s = 0; s < 2; s++) {
         const float* q = o + 2 + 12 * s;
         float* gq = g + 2 + 12 * s;
         float v[4], m = -1e30f;
+        #pragma unroll
         for (int k = 0; k < 4; k++) {
             v[k] = logf(p.w[s][k]) + p.kappa[s][k] * cosf(psis[s] - p.mu[s][k]) - log_i0f(p.kappa[s][k]);
             m = fmaxf(m, v[k]);
         }
         float z = 0.f;
+        #pragma unroll
         for (int k = 0; k < 4; k++) { v[k] = expf(v[k] - m); z += v[k]; }
+        #pragma unroll
         for (int k = 0; k < 4; k++) {
             const float rk = v[k] / z;          // responsibility
             const float kap = p.kappa[s][k], dpsi = psis[s] - p.mu[s][k];

