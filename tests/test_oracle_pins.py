@@ -54,7 +54,7 @@ def test_three_type_enumeration(orc, N):
 @pytest.mark.parametrize("N,fmc,seed,gamma,expect", [
     (10, 1, 42, 1.0, (0, 118, 0)),         # test_fmc_mask default arguments `10 1.0 1`
     (32, 1, 42, 1.0, (0, 6630, 0)),
-    (32, 2, 42, 0.1, (255, 11955, 0)),      # first BASELINE config, seed 42
+    (32, 2, 42, 0.1, (255, 11955, 0)),      # dense PT configuration N=32, seed 42, gamma 0.1
 ])
 def test_fmc_survivor_counts(orc, N, fmc, seed, gamma, expect):
     w = orc.omega(N, fmc, seed)
