@@ -127,30 +127,6 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def host_exchange(E, perm, st, beta_sched, nrep, rep_off, ex_acc, ex_prop):
-    """parallel_tempering.cu:316-352 for all samples at once (vectorised over
-    samples; t and r in the reference's order; drand48 drawn only when the
-    exchange is not accepted outright)."""
-    S = perm.shape[0]
-    idx = np.arange(S)
-    for t in range(NT - 1):
-        db = beta_sched[t] - beta_sched[t + 1]
-        for r in range(nrep):
-            a = perm[:, t * nrep + r]
-            b = perm[:, (t + 1) * nrep + r]
-            delta = db * (E[rep_off + a] - E[rep_off + b])
-            ok = delta >= 0.0
-            need = ~ok
-            if need.any():
-                st[need] = (st[need] * np.uint64(0x5DEECE66D) + np.uint64(0xB)) & np.uint64(0xFFFFFFFFFFFF)
-                u = st[need].astype(np.float64) * (1.0 / 281474976710656.0)
-                ok[need] = u < np.exp(delta[need])
-            ex_prop[:, t] += 1
-            ex_acc[ok, t] += 1
-            sw = idx[ok]
-            perm[sw, t * nrep + r], perm[sw, (t + 1) * nrep + r] = b[ok], a[ok]
-
-
 def run_engine(args, rank, world, device, dist):
     import torch
     import cuda_pspin_b200 as ps
@@ -236,7 +212,7 @@ def run_engine(args, rank, world, device, dist):
     p_host = pin(R_tot, torch.int64)
     S = len(Ns)
     rep_off = np.arange(S, dtype=np.int64) * (NT * NREP_T)
-    perm = np.tile(np.arange(NT * NREP_T, dtype=np.int64), (S, 1))
+    perm = np.tile(np.arange(NT * NREP_T, dtype=np.int32), (S, 1))
     st = np.array([((s + 5000) & 0xFFFFFFFF) << 16 | 0x330E for s in seeds], dtype=np.uint64)
     exa = np.zeros((S, NT - 1), np.int64)
     exp_ = np.zeros((S, NT - 1), np.int64)
@@ -251,8 +227,8 @@ def run_engine(args, rank, world, device, dist):
         lib.pspin_set_betas(eng._h, ps._ptr(b_host))
         lib.pspin_sweep(eng._h, 1)
         lib.pspin_get_results(eng._h, ps._ptr(E_host), ps._ptr(a_host), ps._ptr(p_host))
-        host_exchange(E_host, perm, st, beta, NREP_T, rep_off, exa, exp_)
-        rebuild_betas()
+        # the reference's host exchange (parallel_tempering.cu:316-352), in the library, betas rebuilt in place
+        ps.exchange_host(beta, E_host, rep_off, perm, st, exa, exp_, b_host)
 
     rebuild_betas()
     for _ in range(args.warmup):
@@ -272,7 +248,7 @@ def run_engine(args, rank, world, device, dist):
     e2e = {"value": total_moves / e2e_s, "unit": "pair-moves/s", "h2d_bytes_per_step": 8 * R_tot * sps,
            "d2h_bytes_per_step": 24 * R_tot * sps,
            "loop": "per sweep: pspin_set_betas (H2D, pinned) + pspin_sweep + pspin_get_results (D2H, pinned) "
-                   "+ host exchange (drand48, parallel_tempering.cu:316-352)"}
+                   "+ pspin_exchange_host (drand48, parallel_tempering.cu:316-352, OpenMP over samples)"}
     eng.free()
 
     out = {

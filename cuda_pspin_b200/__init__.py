@@ -124,6 +124,8 @@ def load_library() -> ctypes.CDLL:
         "pspin_resync_drift": (ctypes.c_int, [vp, vp]),
         "pspin_checkpoint_save": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "pspin_pt_shape": (ctypes.c_int, [vp, vp, vp, vp]),
+        "pspin_exchange_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp,
+                                               vp]),
         "pspin_checkpoint_load": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "pspin_observe_get": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int]),
         "pspin_learn_init": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_float]),
@@ -489,6 +491,25 @@ def mc_compute_split_energies(state: Engine):
 
 
 mc_sparse_compute_split_energies = mc_compute_split_energies
+
+
+def exchange_host(beta_sched, energy, rep_off, perm, drand_state, ex_acc, ex_prop, betas=None) -> None:
+    """The reference's host-side replica exchange (parallel_tempering.cu:316-352)
+    in place on caller arrays: perm int32 [S, NT*nrep], drand_state uint64 [S],
+    ex_acc / ex_prop int64 [S, NT-1], energy / betas float64 indexed by
+    rep_off[k] + physical replica."""
+    S, NTn = perm.shape
+    NT = len(beta_sched)
+    for a, dt in ((perm, np.int32), (drand_state, np.uint64), (ex_acc, np.int64), (ex_prop, np.int64),
+                  (energy, np.float64), (rep_off, np.int64)):
+        if a.dtype != dt or not a.flags.c_contiguous:
+            raise TypeError("exchange_host: arrays must be C-contiguous with the documented dtypes")
+    bs = np.ascontiguousarray(beta_sched, np.float64)
+    if betas is not None and (betas.dtype != np.float64 or not betas.flags.c_contiguous):
+        raise TypeError("exchange_host: betas must be C-contiguous float64")
+    _check(load_library().pspin_exchange_host(S, NT, NTn // NT, _ptr(bs), _ptr(energy), _ptr(rep_off), _ptr(perm),
+                                              _ptr(drand_state), _ptr(ex_acc), _ptr(ex_prop),
+                                              None if betas is None else _ptr(betas)))
 
 
 def fmc_mask(N: int, omega, gamma: float):

@@ -1580,6 +1580,46 @@ extern "C" int pspin_observe_get(pspin_state* s, int64_t* n_rows, double* energy
     return PSPIN_OK;
 }
 
+// Host-side exchange for drivers that keep the PT loop on the host, as the
+// reference's driver does (parallel_tempering.cu:316-352): t from the hottest
+// pair up, a swap applied before the next t, drand48 drawn only when delta < 0,
+// then betas rebuilt from perm (:347-351).  Samples are independent (OpenMP).
+extern "C" int pspin_exchange_host(int n_samples, int NT, int nrep, const double* beta_sched, const double* energy,
+                                   const int64_t* rep_off, int32_t* perm, uint64_t* drand_state, int64_t* ex_acc,
+                                   int64_t* ex_prop, double* betas) {
+    if (n_samples < 0 || NT < 2 || nrep < 1 || !beta_sched || !energy || !rep_off || !perm || !drand_state ||
+        !ex_acc || !ex_prop)
+        return fail(PSPIN_ERR_ARG, "pspin_exchange_host: bad arguments");
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n_samples; k++) {
+        int32_t* pm = perm + (size_t)k * NT * nrep;
+        const double* E = energy + rep_off[k];
+        uint64_t st = drand_state[k];
+        int64_t* acc = ex_acc + (size_t)k * (NT - 1);
+        int64_t* prop = ex_prop + (size_t)k * (NT - 1);
+        for (int t = 0; t < NT - 1; t++) {
+            const double db = beta_sched[t] - beta_sched[t + 1];
+            for (int r = 0; r < nrep; r++) {
+                const int32_t a = pm[t * nrep + r], b = pm[(t + 1) * nrep + r];
+                const double delta = db * (E[a] - E[b]);
+                prop[t]++;
+                bool ok = delta >= 0.0;
+                if (!ok) ok = drand48_next(st) < std::exp(delta);
+                if (ok) {
+                    acc[t]++;
+                    pm[t * nrep + r] = b;
+                    pm[(t + 1) * nrep + r] = a;
+                }
+            }
+        }
+        drand_state[k] = st;
+        if (betas)
+            for (int t = 0; t < NT; t++)
+                for (int r = 0; r < nrep; r++) betas[rep_off[k] + pm[t * nrep + r]] = beta_sched[t];
+    }
+    return PSPIN_OK;
+}
+
 extern "C" int pspin_pt_shape(pspin_state* s, int* NT, int* nrep_per_temp, int* pt_freq) {
     if (!s) return fail(PSPIN_ERR_ARG, "null handle");
     if (NT) *NT = s->pt_NT;

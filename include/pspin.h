@@ -170,6 +170,15 @@ int  pspin_pt_run(pspin_state* s, int nsweeps);
  * cumulative exchange counters [NT-1] of one sample. */
 int  pspin_pt_get(pspin_state* s, int sample, int32_t* perm, int64_t* ex_acc, int64_t* ex_prop);
 int  pspin_pt_sweeps_done(pspin_state* s, int64_t* sweeps);
+/* Host-side replica exchange for drivers that keep the PT loop on the host
+ * (the reference's driver pattern, parallel_tempering.cu:316-352) on arrays
+ * the caller owns: energy[] and betas[] indexed by rep_off[k] + physical
+ * replica, perm[S][NT*nrep] (logical t*nrep+r -> physical), drand_state[S]
+ * (48-bit drand48 states, srand48(seed+5000) for the reference's stream),
+ * counters ex_acc/ex_prop[S][NT-1]; betas (or NULL) rebuilt from perm. */
+int  pspin_exchange_host(int n_samples, int NT, int nrep, const double* beta_sched, const double* energy,
+                         const int64_t* rep_off, int32_t* perm, uint64_t* drand_state, int64_t* ex_acc,
+                         int64_t* ex_prop, double* betas);
 /* NT, replicas per temperature and exchange period set by pspin_pt_init (0s before). */
 int  pspin_pt_shape(pspin_state* s, int* NT, int* nrep_per_temp, int* pt_freq);
 /* Block-shape autotuner (no reference counterpart): times `sweeps` sweeps

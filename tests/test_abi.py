@@ -6,6 +6,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -59,3 +60,38 @@ def test_bad_arguments_return_codes(ps):
     lib = ps.load_library()
     assert lib.pspin_create_batch(None, 0, 0, None, None) == 1
     assert lib.pspin_destroy(None) == 0
+
+
+def test_host_exchange_matches_oracle(ps, orc):
+    """pspin_exchange_host (the reference's host PT exchange, parallel_tempering.cu:316-352)
+    equals the oracle's exchange, sample by sample, over many steps."""
+    import ctypes
+    rng = np.random.default_rng(3)
+    S, NT, nr = 5, 6, 3
+    beta = 1.0 / np.geomspace(1.5, 0.3, NT)
+    rep_off = (np.arange(S, dtype=np.int64) * NT * nr)
+    perm = np.tile(np.arange(NT * nr, dtype=np.int32), (S, 1))
+    st = np.array([orc_srand(orc, 100 + k + 5000) for k in range(S)], np.uint64)
+    acc = np.zeros((S, NT - 1), np.int64)
+    prop = np.zeros((S, NT - 1), np.int64)
+    betas = np.zeros(S * NT * nr)
+    ref = [(perm[k].copy(), st[k:k + 1].copy(), np.zeros(NT - 1, np.int64), np.zeros(NT - 1, np.int64))
+           for k in range(S)]
+    for step in range(50):
+        E = rng.normal(0, 3.0, S * NT * nr)
+        ps.exchange_host(beta, E, rep_off, perm, st, acc, prop, betas)
+        for k in range(S):
+            p, s_, a_, pr_ = ref[k]
+            bo = np.zeros(NT * nr)
+            Ek = np.ascontiguousarray(E[k * NT * nr:(k + 1) * NT * nr])
+            orc.lib().orc_exchange(NT, nr, orc.P(beta), orc.P(Ek), orc.P(p), orc.P(s_), orc.P(a_), orc.P(pr_),
+                                   orc.P(bo))
+            np.testing.assert_array_equal(perm[k], p)
+            assert st[k] == s_[0]
+            np.testing.assert_array_equal(acc[k], a_)
+            np.testing.assert_array_equal(betas[k * NT * nr:(k + 1) * NT * nr], bo)
+    assert acc.sum() > 0 and (prop == 50 * nr).all()
+
+
+def orc_srand(orc, seed):
+    return int(orc.lib().orc_srand48_state(seed))
