@@ -24,7 +24,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "noalloc.cu", "sweep_cluster.cu", "sweep_resident.cu", "tcfield.cu", "learned.cu", "layout.cpp"]
+LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "noalloc.cu", "sweep_cluster.cu", "sweep_resident.cu", "analysis.cu", "tcfield.cu", "learned.cu", "layout.cpp"]
 CUTLASS = "/opt/prime-rl/.venv/lib/python3.12/site-packages/flashinfer/data/cutlass"
 DRIVERS = {
     "pspin_pt": ["drivers/pt_main.cpp"],

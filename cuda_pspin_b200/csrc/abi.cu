@@ -1584,6 +1584,19 @@ extern "C" int pspin_observe_get(pspin_state* s, int64_t* n_rows, double* energy
 // reference's driver does (parallel_tempering.cu:316-352): t from the hottest
 // pair up, a swap applied before the next t, drand48 drawn only when delta < 0,
 // then betas rebuilt from perm (:347-351).  Samples are independent (OpenMP).
+extern "C" int pspin_overlap_counts_impl(int N, int NT, int nrep, int nsnap, const double* configs, int nbins,
+                                         double qmin, double qmax, long long* counts, const char** err);
+
+extern "C" int pspin_overlap_counts(int N, int NT, int nrep, int nsnap, const double* configs, int nbins, double qmin,
+                                    double qmax, int64_t* counts) {
+    const char* err = nullptr;
+    const int rc = pspin_overlap_counts_impl(N, NT, nrep, nsnap, configs, nbins, qmin, qmax,
+                                             reinterpret_cast<long long*>(counts), &err);
+    if (rc == 1) return fail(PSPIN_ERR_ARG, "%s", err);
+    if (rc) return fail(PSPIN_ERR_CUDA, "overlap counts: %s", err);
+    return PSPIN_OK;
+}
+
 extern "C" int pspin_exchange_host(int n_samples, int NT, int nrep, const double* beta_sched, const double* energy,
                                    const int64_t* rep_off, int32_t* perm, uint64_t* drand_state, int64_t* ex_acc,
                                    int64_t* ex_prop, double* betas) {

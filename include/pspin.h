@@ -179,6 +179,14 @@ int  pspin_pt_sweeps_done(pspin_state* s, int64_t* sweeps);
 int  pspin_exchange_host(int n_samples, int NT, int nrep, const double* beta_sched, const double* energy,
                          const int64_t* rep_off, int32_t* perm, uint64_t* drand_state, int64_t* ex_acc,
                          int64_t* ex_prop, double* betas);
+/* Overlap histogram counts of one sample's saved configurations on the GPU
+ * (the Parisi P(q) loop of analysis_pt.cpp:1337-1437): configs
+ * [nsnap][NT][nrep][N][2] doubles (configs.bin records without the sweep
+ * numbers), counts [NT][nbins] of q_ab = Re sum_k a_k conj(b_k) / N over all
+ * snapshots and pairs a < b, binned as the reference bins (same rounding, so
+ * the same bins). */
+int  pspin_overlap_counts(int N, int NT, int nrep, int nsnap, const double* configs, int nbins, double qmin,
+                          double qmax, int64_t* counts);
 /* NT, replicas per temperature and exchange period set by pspin_pt_init (0s before). */
 int  pspin_pt_shape(pspin_state* s, int* NT, int* nrep_per_temp, int* pt_freq);
 /* Block-shape autotuner (no reference counterpart): times `sweeps` sweeps
