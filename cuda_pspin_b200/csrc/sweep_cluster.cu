@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     const int total = P.nsweeps * steps;
     const int TW = C * W, gw = (int)rank * W + warp;
 
-    Stream<2> st;
+    Stream<2, false> st;
     st.key0 = S.pair_key0;
     st.key1 = S.pair_key1;
     st.N = N;

@@ -98,8 +98,11 @@ struct Cursor {
 };
 
 // kLists: lists visited per move -- sites i0, j0 (2); then, for the two-pass
-// sweep, the pair's two sub-lists (4)
-template <int kLists>
+// sweep, the pair's two sub-lists (4).  kCache: keep the last pair pick of the
+// consumer and of the cursor (fewer Philox evaluations, two more live
+// registers; measured faster for sweep_kernel and the two-pass sweep, slower
+// for the cluster sweep)
+template <int kLists, bool kCache = true>
 struct Stream {
     uint32_t key0, key1;
     int N;
@@ -107,31 +110,44 @@ struct Stream {
     const int* pair_chunks;   // this sample's N(N-1)*(kSplit+1) pair sub-list chunk indices
     long long sweep0;
     int steps, total, part0, part1;
+    // the last pair pick of the consumer (slot 0) and of the prefetch cursor
+    // (slot 1): each list lookup of a move reuses it instead of another Philox
+    int cm[2] = {-1, -1}, ci[2] = {0, 0}, cj[2] = {0, 0};
 
-    __device__ __forceinline__ void range(int m, int which, int& c, int& c_end) const {
+    __device__ __forceinline__ void range(int m, int which, int& c, int& c_end, int slot = 0) {
         int i0, j0;
-        const long long sw = sweep0 + m / steps;
-        pair_pick(key0, key1, (uint64_t)sw, (uint32_t)(m % steps), N, i0, j0);
+        if (kCache) {
+            if (m != cm[slot]) {
+                const long long sw = sweep0 + m / steps;
+                pair_pick(key0, key1, (uint64_t)sw, (uint32_t)(m % steps), N, ci[slot], cj[slot]);
+                cm[slot] = m;
+            }
+            i0 = ci[slot];
+            j0 = cj[slot];
+        } else {
+            const long long sw = sweep0 + m / steps;
+            pair_pick(key0, key1, (uint64_t)sw, (uint32_t)(m % steps), N, i0, j0);
+        }
         const int* sc = (kLists == 2 || which < 2) ? site_chunks + ((which & 1) ? j0 : i0) * (kSplit + 1)
                                                    : pair_chunks + (2 * (j0 * (j0 - 1) / 2 + i0) + (which & 1)) * (kSplit + 1);
         c = __ldg(sc + part0);
         c_end = __ldg(sc + part1);
     }
     // move to the next chunk (skipping empty ranges); m == total at the end
-    __device__ __forceinline__ void next(Cursor& k) const {
+    __device__ __forceinline__ void next(Cursor& k) {
         k.c++;
         while (k.c >= k.c_end) {
             if (++k.which == kLists) {
                 k.which = 0;
                 if (++k.m >= total) return;
             }
-            range(k.m, k.which, k.c, k.c_end);
+            range(k.m, k.which, k.c, k.c_end, 1);
         }
     }
-    __device__ __forceinline__ Cursor first() const {
+    __device__ __forceinline__ Cursor first() {
         Cursor k{0, 0, 0, 0};
         if (total <= 0) return k;
-        range(0, 0, k.c, k.c_end);
+        range(0, 0, k.c, k.c_end, 1);
         k.c--;
         next(k);
         return k;
