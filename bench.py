@@ -136,7 +136,10 @@ def run_engine(args, rank, world, device, dist):
     cfgs = [ps.default_config(N=N, nrep=NT * NREP_T, seed=s, fmc_mode=0, T=float(T[0]))
             for N, s in zip(Ns, seeds)]
     t_setup = time.perf_counter()
-    eng = ps.Engine(cfgs, ps.PSPIN_DENSE, ps.make_options(resync_every=1024))
+    shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else None
+    opts = ps.make_options(resync_every=1024, warps_per_unit=shape[0] if shape else 0,
+                           cluster_size=(shape[1] if shape[1] > 0 else -1) if shape else 0)
+    eng = ps.Engine(cfgs, ps.PSPIN_DENSE, opts)
     t_setup = time.perf_counter() - t_setup
     eng.pt_init(NT, NREP_T, beta, 1)
     sps = args.sweeps_per_step
@@ -149,7 +152,10 @@ def run_engine(args, rank, world, device, dist):
         eng.pt_run(sps)
     # block shape by the engine's autotuner (state restored after its trials),
     # then one more step so the PT graph is captured with that shape
-    tuned_w, tuned_c, tuned_ms = eng.autotune(2)
+    if shape:
+        tuned_w, tuned_c = shape
+    else:
+        tuned_w, tuned_c, tuned_ms = eng.autotune(2)
     eng.pt_run(sps)
     eng.get_profile()                  # zero the launch counters
     ext = torch.cuda.ExternalStream(eng.stream_ptr(), device=device)
@@ -263,7 +269,7 @@ def run_engine(args, rank, world, device, dist):
                    "l2": f"inputs exceed L2: {entries * 8 / 1e9:.2f} GB of site lists per GPU (no flush)",
                    "parallelism": f"samples sharded, {world} GPU(s), no collective",
                    "block_shape": {"warps_per_cta": tuned_w, "ctas_per_replica_block": tuned_c,
-                                   "chosen_by": "pspin_autotune (2 sweeps per shape)"},
+                                   "chosen_by": "--shape" if shape else "pspin_autotune (2 sweeps per shape)"},
                    "launch": "sweep + exchange per PT step, replayed as CUDA graphs of 32 steps",
                    "setup_s": t_setup},
         "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
@@ -296,6 +302,8 @@ def main():
     ap.add_argument("--sweeps-per-step", type=int, default=16)
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default="", help="W,C: warps per CTA, CTAs per replica block (skips the autotuner; "
+                                                "for profiling a fixed kernel shape)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
