@@ -199,7 +199,11 @@ def run_engine(args, rank, world, device, dist):
     tf = os.path.join(ROOT, "profiles", "sweep_dense_batched_traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get("bytes_per_launch")
+            rec = json.load(open(tf))
+            # the capture of the kernel this launch ran: cluster split or one CTA
+            if tuned_c == 1 and "one_cta_kernel" in rec:
+                rec = rec["one_cta_kernel"]
+            traffic = None if tuned_c == 0 else rec.get("bytes_per_launch")
         except Exception:
             traffic = None
     executed = None   # executed FP32 ops per launch: 4 per data entry and replica + group/proposal overhead
