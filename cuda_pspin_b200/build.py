@@ -30,6 +30,7 @@ DRIVERS = {
     "pspin_pt": ["drivers/pt_main.cpp"],
     "pspin_pt_sparse": ["drivers/pt_sparse_main.cpp"],
     "pspin_mc": ["drivers/mc_main.cpp"],
+    "pspin_sa": ["drivers/sa_main.cpp"],
 }
 
 

@@ -347,6 +347,159 @@ int pt_main(int argc, char** argv, int variant) {
     return 0;
 }
 
+int sa_main(int argc, char** argv) {
+    // simulated_annealing.cu:32-70: SA flags, the rest for parse_args
+    double Tmax = -1.0, Tmin = -1.0;
+    int ntemp = -1, batch = 1;
+    std::vector<char*> rest;
+    rest.push_back(argv[0]);
+    for (int i = 1; i < argc; i++) {
+        if (!strcmp(argv[i], "-Tmax") && i + 1 < argc) Tmax = atof(argv[++i]);
+        else if (!strcmp(argv[i], "-Tmin") && i + 1 < argc) Tmin = atof(argv[++i]);
+        else if (!strcmp(argv[i], "-ntemp") && i + 1 < argc) ntemp = atoi(argv[++i]);
+        else if (!strcmp(argv[i], "-batch") && i + 1 < argc) batch = atoi(argv[++i]);
+        else rest.push_back(argv[i]);
+    }
+    if (Tmax < 0 || Tmin < 0 || ntemp < 1) {
+        fprintf(stderr, "Simulated Annealing requires: -Tmax tmax -Tmin tmin -ntemp nt\n");
+        fprintf(stderr, "Usage: %s -N n -Tmax tmax -Tmin tmin -ntemp nt -iter k "
+                        "[-nrep n] [-J j] [-seed s] [-save_freq f] [-label l] [-dev d] "
+                        "[-fmc 0|1|2] [-gamma g] [-verbose [0|1|2]] [-batch K]\n", argv[0]);
+        return 1;
+    }
+    if (Tmin > Tmax) {
+        fprintf(stderr, "Error: Tmin (%.4f) > Tmax (%.4f)\n", Tmin, Tmax);
+        return 1;
+    }
+    if (batch < 1) {
+        fprintf(stderr, "Error: -batch must be >= 1\n");
+        return 1;
+    }
+    pspin_config cfg;
+    if (pspin_parse_args((int)rest.size(), rest.data(), &cfg) != PSPIN_OK) {
+        fprintf(stderr, "%s\n", pspin_last_error());
+        return 1;
+    }
+    if (cfg.mc_iterations < 0 || cfg.mc_iterations > 30) {
+        fprintf(stderr, "Error: -iter k gives 2^k sweeps per temperature; k must be in [0, 30]\n");
+        return 1;
+    }
+    const int sweeps_per_temp = 1 << cfg.mc_iterations;    // :72
+    const int N = cfg.N, nrep = cfg.nrep;
+    cfg.T = Tmax;                                           // :173
+
+    // one data directory per sample, data/SA_N{N}_NR{nrep}_S{label} (:83-100)
+    const int label0 = (cfg.label >= 0) ? cfg.label : 0;
+    std::vector<pspin_config> cfgs(batch, cfg);
+    std::vector<std::string> dirs(batch);
+    std::vector<FILE*> fouts(batch, nullptr);
+    mkdir("data", 0755);
+    for (int k = 0; k < batch; k++) {
+        cfgs[k].seed = cfg.seed + (uint64_t)k;
+        cfgs[k].label = label0 + k;
+        char datadir[256];
+        snprintf(datadir, sizeof(datadir), "data/SA_N%d_NR%d_S%d", N, nrep, label0 + k);
+        mkdir(datadir, 0755);
+        dirs[k] = datadir;
+        mkdir((dirs[k] + "/configs").c_str(), 0755);
+        fouts[k] = fopen((dirs[k] + "/energy_accept.txt").c_str(), "w");
+        if (!fouts[k]) {
+            fprintf(stderr, "Cannot open %s/energy_accept.txt\n", datadir);
+            return 2;
+        }
+        fprintf(fouts[k], "# T\tsweep");
+        for (int r = 0; r < nrep; r++) fprintf(fouts[k], "\tE%d/N\tacc%d", r, r);
+        fprintf(fouts[k], "\n");
+    }
+
+    printf("\n  p-Spin 2+4 :: Simulated Annealing (B200 engine)\n");
+    pspin_options opt;
+    memset(&opt, 0, sizeof(opt));
+    opt.trace_replica = -1;
+    pspin_state* st = nullptr;
+    if (!check(pspin_create_batch(cfgs.data(), batch, PSPIN_DENSE, &opt, &st))) return 1;
+    if (cfg.fmc_mode > 0) {                                 // :176-194
+        for (int k = 0; k < batch; k++) {
+            std::vector<double> w(N);
+            if (!check(pspin_get_omega(st, k, w.data()))) return 1;
+            FILE* ff = fopen((dirs[k] + "/frequencies.txt").c_str(), "w");
+            if (ff) {
+                fprintf(ff, "# i omega_i\n");
+                for (int i = 0; i < N; i++) fprintf(ff, "%d\t%.12f\n", i, w[i]);
+                fclose(ff);
+            }
+        }
+    }
+
+    const int R_all = batch * nrep;
+    std::vector<double> E(R_all), spins((size_t)R_all * N * 2);
+    std::vector<int64_t> acc(R_all), prop(R_all);
+    const double t0 = now_s();
+    // geometric cooling T_k = Tmax A^k, A = (Tmin/Tmax)^(1/(ntemp-1)) (:207-208, :218-220)
+    const double A = (ntemp > 1) ? pow(Tmin / Tmax, 1.0 / (ntemp - 1)) : 1.0;
+    printf("  %-22s %.8f\n", "schedule (A)", A);
+    for (int step = 0; step < ntemp; step++) {
+        const double T = Tmax * pow(A, step);
+        // mc_sweep refills every beta with 1/T before each sweep (mc.cu:749-752);
+        // T is fixed within a step, so one fill per step is the same
+        if (!check(pspin_fill_betas(st, 1.0 / T))) return 1;
+        if (!check(pspin_reset_counters(st))) return 1;     // :223-224
+        int s = 0;
+        while (s < sweeps_per_temp) {
+            int next = s;
+            while (!((next + 1) % cfg.save_freq == 0 || next == sweeps_per_temp - 1)) next++;
+            if (!check(pspin_sweep(st, next - s + 1))) return 1;
+            s = next;
+            if (!check(pspin_get_results(st, E.data(), acc.data(), prop.data()))) return 1;
+            for (int k = 0; k < batch; k++) {               // :238-246
+                fprintf(fouts[k], "%.8f\t%d", T, s + 1);
+                for (int r = 0; r < nrep; r++) {
+                    const int i = k * nrep + r;
+                    const double a = (prop[i] > 0) ? (double)acc[i] / prop[i] : 0.0;
+                    fprintf(fouts[k], "\t%.8f\t%.5f", E[i] / N, a);
+                }
+                fprintf(fouts[k], "\n");
+                fflush(fouts[k]);
+            }
+            if (!check(pspin_reset_counters(st))) return 1; // :268-270
+            s++;
+        }
+        if (step >= ntemp / 2) {                            // :274-292
+            if (!check(pspin_get_spins(st, spins.data()))) return 1;
+            for (int k = 0; k < batch; k++)
+                for (int r = 0; r < nrep; r++) {
+                    char conffile[512];
+                    snprintf(conffile, sizeof(conffile), "%s/configs/conf_r%d_T%.6f.bin", dirs[k].c_str(), r, T);
+                    FILE* fc = fopen(conffile, "wb");
+                    if (fc) {
+                        fwrite(&spins[(size_t)(k * nrep + r) * N * 2], sizeof(double), 2 * (size_t)N, fc);
+                        fclose(fc);
+                    }
+                }
+        }
+        if (cfg.verbose == 1) {
+            printf("  [%d/%d] T=%.6f", step + 1, ntemp, T);
+            for (int r = 0; r < nrep; r++) printf("  E/N=%.4f", E[r] / N);
+            printf("\n");
+        }
+    }
+    const double elapsed = now_s() - t0;
+    printf("\n  %-22s %.3f s\n", "total time", elapsed);
+    printf("  %-22s %d x %d = %lld\n", "total sweeps", ntemp, sweeps_per_temp, (long long)ntemp * sweeps_per_temp);
+    printf("  %-22s %d\n", "samples", batch);
+    for (int k = 0; k < batch; k++) {                       // :307-315
+        FILE* ftim = fopen((dirs[k] + "/time.txt").c_str(), "w");
+        if (ftim) {
+            fprintf(ftim, "# N nrep ntemp sweeps_per_temp Tmax Tmin total_time_s\n");
+            fprintf(ftim, "%d %d %d %d %.6f %.6f %.6f\n", N, nrep, ntemp, sweeps_per_temp, Tmax, Tmin, elapsed);
+            fclose(ftim);
+        }
+        fclose(fouts[k]);
+    }
+    pspin_destroy(st);
+    return 0;
+}
+
 int mc_main(int argc, char** argv) {
     pspin_config cfg;
     if (pspin_parse_args(argc, argv, &cfg) != PSPIN_OK) {

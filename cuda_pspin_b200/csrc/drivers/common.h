@@ -8,3 +8,5 @@
 int pt_main(int argc, char** argv, int variant);
 // montecarlo.cu:23-231
 int mc_main(int argc, char** argv);
+// simulated_annealing.cu:30-314; extension: -batch K samples in one engine
+int sa_main(int argc, char** argv);

@@ -142,3 +142,95 @@ def test_gpu_overlap_distribution_matches_analysis_pt(tmp_path):
         assert abs(x[1] - y[1]) <= 1e-12 * max(1.0, abs(y[1])) and abs(x[2] - y[2]) <= 1e-9 * max(1.0, abs(y[2]))
         n_rows += 1
     assert n_rows == 4 * 100
+
+
+SA_FLAGS = ["-N", "12", "-nrep", "3", "-Tmax", "1.6", "-Tmin", "0.3", "-ntemp", "5", "-iter", "6", "-save_freq", "16",
+            "-seed", "9", "-fmc", "2", "-gamma", "0.3", "-label", "2"]
+
+
+def test_sa_driver_matches_reference_files(tmp_path):
+    """pspin_sa against the reference's simulated_annealing: same directory,
+    same frequencies.txt and time.txt header, the same energy_accept.txt
+    header, rows, temperature and sweep columns, and the same configuration
+    files (second half of the schedule, conf_r{r}_T{T}.bin)."""
+    ours, ref = tmp_path / "ours", tmp_path / "ref"
+    ours.mkdir()
+    ref.mkdir()
+    run([os.path.join(BIN, "pspin_sa"), *SA_FLAGS], ours)
+    run([os.path.join(REF, "simulated_annealing"), *SA_FLAGS], ref)
+    d_o, d_r = the_dir(ours), the_dir(ref)
+    assert os.path.basename(d_o) == os.path.basename(d_r) == "SA_N12_NR3_S2"
+    assert sorted(os.listdir(d_o)) == sorted(os.listdir(d_r))
+    assert open(os.path.join(d_o, "frequencies.txt")).read() == open(os.path.join(d_r, "frequencies.txt")).read()
+    assert open(os.path.join(d_o, "time.txt")).readline() == open(os.path.join(d_r, "time.txt")).readline()
+    t_o = open(os.path.join(d_o, "time.txt")).read().split("\n")[1].split()[:6]
+    t_r = open(os.path.join(d_r, "time.txt")).read().split("\n")[1].split()[:6]
+    assert t_o == t_r                                                # N nrep ntemp sweeps/T Tmax Tmin
+    h_o, r_o = table(os.path.join(d_o, "energy_accept.txt"))
+    h_r, r_r = table(os.path.join(d_r, "energy_accept.txt"))
+    assert h_o == h_r
+    assert [x[:2] for x in r_o] == [x[:2] for x in r_r]              # T (%.8f) and sweep columns
+    assert [len(x) for x in r_o] == [len(x) for x in r_r]
+    confs = sorted(os.listdir(os.path.join(d_r, "configs")))
+    assert len(confs) == 3 * 3 and sorted(os.listdir(os.path.join(d_o, "configs"))) == confs
+    for f in confs:
+        a = np.fromfile(os.path.join(d_o, "configs", f), np.float64)
+        b = np.fromfile(os.path.join(d_r, "configs", f), np.float64)
+        assert a.size == b.size == 2 * 12
+        # same initial amplitudes and radius-conserving moves: each replica
+        # stays on the sphere it started on (the reference's initial radius)
+        assert abs(np.sum(a * a) - np.sum(b * b)) < 1e-5 * np.sum(b * b)
+
+
+def test_analysis_sa_reads_engine_output(tmp_path):
+    flags = ["-N", "12", "-nrep", "2", "-Tmax", "1.6", "-Tmin", "0.3", "-ntemp", "4", "-iter", "6",
+             "-save_freq", "16", "-seed", "3", "-label", "0", "-batch", "3"]
+    run([os.path.join(BIN, "pspin_sa"), *flags], tmp_path)
+    assert sorted(os.listdir(tmp_path / "data")) == ["SA_N12_NR2_S0", "SA_N12_NR2_S1", "SA_N12_NR2_S2"]
+    p = run([os.path.join(REF, "analysis_sa"), "-N", "12", "-nrep", "2"], tmp_path)
+    assert "samples" in p.stdout
+    produced = [f for _, _, fs in os.walk(tmp_path / "analysis") for f in fs]
+    assert len(produced) > 0, p.stdout[-2000:]
+
+
+def test_sa_statistics_match_reference(tmp_path):
+    """Annealing the same 32 disorder samples (seeds 100..131, identical
+    couplings and initial amplitudes) with pspin_sa -batch 32 and with 32 runs
+    of the reference's simulated_annealing: for every temperature of the
+    schedule, the mean over samples of (engine - reference) of the
+    second-half window averages of E/N and of the acceptance is compared
+    with its standard error.  The per-replica chains have the same law on
+    both sides (the engine shares one pair schedule among a sample's
+    replicas), so the paired z-scores are standard normal: every |z| < 3.5
+    and at least 80 % within 2 sigma."""
+    S, nrep, ntemp, it, save = 32, 4, 6, 9, 64
+    flags = ["-N", "12", "-nrep", str(nrep), "-Tmax", "1.6", "-Tmin", "0.3", "-ntemp", str(ntemp),
+             "-iter", str(it), "-save_freq", str(save)]
+    ours, ref = tmp_path / "ours", tmp_path / "ref"
+    ours.mkdir()
+    ref.mkdir()
+    run([os.path.join(BIN, "pspin_sa"), *flags, "-seed", "100", "-label", "0", "-batch", str(S)], ours)
+    for k in range(S):
+        run([os.path.join(REF, "simulated_annealing"), *flags, "-seed", str(100 + k), "-label", str(k)], ref)
+
+    def observables(path):
+        rows = np.loadtxt(os.path.join(path, "energy_accept.txt"))
+        Ts = np.unique(rows[:, 0])[::-1]
+        assert len(Ts) == ntemp
+        out = np.zeros((2, ntemp))
+        for t, T in enumerate(Ts):
+            blk = rows[(rows[:, 0] == T) & (rows[:, 1] > (1 << it) // 2)]
+            out[0, t] = blk[:, 2::2].mean()
+            out[1, t] = blk[:, 3::2].mean()
+        return out
+
+    names = [f"SA_N12_NR{nrep}_S{k}" for k in range(S)]
+    obs_o = np.array([observables(str(ours / "data" / n)) for n in names])
+    obs_r = np.array([observables(str(ref / "data" / n)) for n in names])
+    diff = obs_o - obs_r
+    z = diff.mean(axis=0) / (diff.std(axis=0, ddof=1) / np.sqrt(S))
+    print("paired z (E/N, acc) per T:", np.round(z, 2).tolist())
+    print("engine E/N per T:", np.round(obs_o[:, 0].mean(axis=0), 4).tolist())
+    print("reference E/N per T:", np.round(obs_r[:, 0].mean(axis=0), 4).tolist())
+    assert np.all(np.abs(z) < 3.5), z
+    assert np.mean(np.abs(z) < 2.0) >= 0.8, z
