@@ -32,13 +32,19 @@ struct LearnParams {
 // tensor cores with warp-level mma.sync m16n8k16 (BF16 operands, FP32
 // accumulation): each layer is Out[32 x units] = In[32 x K] W^T, two m16
 // tiles of replicas x n8 tiles of units, the n8 tiles spread over the warps.
-// A fragments come from the activations in shared memory (layout
-// X[k][32], rounded to BF16), B fragments straight from the BF16 weight rows
-// (two consecutive inputs of one unit are one 32-bit word), bias and tanh in
-// the FP32 epilogue.  K is padded to 16 (first layer) and the 26 outputs to
-// 32 with zeros.  (32 x 64 tiles are below tcgen05's smallest M of 64, and
-// the step is latency-bound.)  Fragment layouts: PTX ISA, "Matrix Fragments
-// for mma.m16n8k16 with floating point type".
+// A fragments come from the activations in shared memory, stored already
+// rounded to BF16 with two consecutive inputs of one replica in one 32-bit
+// word (row kp holds inputs 2kp, 2kp+1 of the 32 replicas; row stride
+// kActStride = 40 words, so the 8 row groups x 4 column pairs of a fragment
+// load hit 32 distinct banks).  B fragments come straight from the BF16
+// weight rows in global memory (12.9 KB, L1-resident; two consecutive
+// inputs of one unit are one 32-bit word).  Bias and tanh in the FP32
+// epilogue, which packs the lane's two units back into one word.  K is
+// padded to 16 (first layer) and the 26 outputs to 32 with zeros; the
+// outputs stay FP32 (row stride kOutStride).  (32 x 64 tiles are below
+// tcgen05's smallest M of 64, and the step is latency-bound.)  Fragment
+// layouts: PTX ISA, "Matrix Fragments for mma.m16n8k16 with floating point
+// type".
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<uint32_t*>(&v);
@@ -53,11 +59,15 @@ __device__ __forceinline__ void mma_bf16_16816(float* d, uint32_t a0, uint32_t a
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// One layer: X [K][32] floats in shared memory -> Y [units][32];
-// weights w[u*K + k] (BF16), bias bias[u]; act: tanh
-template <int K, int UNITS, bool ACT>
+constexpr int kActStride = 40;    // words per packed activation row (32 replicas + 8 pad)
+constexpr int kOutStride = 36;    // floats per output row (32 replicas + 4 pad)
+
+// One layer: X [ceil(K/2)][kActStride] packed BF16 pairs in shared memory ->
+// Y, packed the same way (HIDDEN: tanh) or FP32 [units][kOutStride] (the
+// output layer); weights w[u*K + k] (BF16, global), bias bias[u]
+template <int K, int UNITS, bool HIDDEN>
 __device__ __forceinline__ void mlp_layer_mma(const __nv_bfloat16* __restrict__ w, const __nv_bfloat16* __restrict__ bias,
-                                              const float* X, float* Y, int warp, int W, int lane) {
+                                              const uint32_t* X, void* Y, int warp, int W, int lane) {
     constexpr int KP = K < 16 ? 16 : K;          // padded K
     constexpr int NT = (UNITS + 7) / 8;          // n8 tiles
     const int g = lane >> 2, t = lane & 3;
@@ -66,70 +76,91 @@ __device__ __forceinline__ void mlp_layer_mma(const __nv_bfloat16* __restrict__ 
         float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
 #pragma unroll
         for (int k0 = 0; k0 < KP; k0 += 16) {
-            const int ka = k0 + 2 * t, kb = k0 + 2 * t + 8;
+            const int ka = k0 + 2 * t, kb = ka + 8;
             uint32_t b0 = 0u, b1 = 0u;
             if (u < UNITS) {
-                if (ka < K) b0 = *reinterpret_cast<const uint32_t*>(w + u * K + ka);
-                if (kb < K) b1 = *reinterpret_cast<const uint32_t*>(w + u * K + kb);
+                if (ka < K) b0 = __ldg(reinterpret_cast<const unsigned int*>(w + u * K + ka));
+                if (kb < K) b1 = __ldg(reinterpret_cast<const unsigned int*>(w + u * K + kb));
             }
+            const uint32_t* xa = X + (ka >> 1) * kActStride;
+            const uint32_t* xb = X + (kb >> 1) * kActStride;
 #pragma unroll
             for (int mt = 0; mt < 2; mt++) {
                 const int r = mt * 16 + g;
-                const float x00 = ka < K ? X[ka * 32 + r] : 0.f, x01 = ka < K ? X[(ka + 1) * 32 + r] : 0.f;
-                const float x10 = ka < K ? X[ka * 32 + r + 8] : 0.f, x11 = ka < K ? X[(ka + 1) * 32 + r + 8] : 0.f;
-                const float x20 = kb < K ? X[kb * 32 + r] : 0.f, x21 = kb < K ? X[(kb + 1) * 32 + r] : 0.f;
-                const float x30 = kb < K ? X[kb * 32 + r + 8] : 0.f, x31 = kb < K ? X[(kb + 1) * 32 + r + 8] : 0.f;
-                mma_bf16_16816(acc[mt], pack_bf16x2(x00, x01), pack_bf16x2(x10, x11), pack_bf16x2(x20, x21),
-                               pack_bf16x2(x30, x31), b0, b1);
+                mma_bf16_16816(acc[mt], ka < K ? xa[r] : 0u, ka < K ? xa[r + 8] : 0u, kb < K ? xb[r] : 0u,
+                               kb < K ? xb[r + 8] : 0u, b0, b1);
             }
         }
-        // epilogue: D element (row g (+8), col 2t (+1)) -> unit nt*8 + 2t (+1), replica mt*16 + g (+8)
+        // epilogue: D element (row g (+8), col 2t (+1)) -> unit u0 (+1), replica mt*16 + g (+8)
         const int u0 = nt * 8 + 2 * t;
+        const float bb0 = u0 < UNITS ? __bfloat162float(bias[u0]) : 0.f;
+        const float bb1 = u0 + 1 < UNITS ? __bfloat162float(bias[u0 + 1]) : 0.f;
 #pragma unroll
-        for (int c = 0; c < 2; c++) {
-            const int uu = u0 + c;
-            if (uu < UNITS) {
-                const float bb = __bfloat162float(bias[uu]);
-#pragma unroll
-                for (int mt = 0; mt < 2; mt++) {
-                    float z0 = acc[mt][c] + bb, z1 = acc[mt][2 + c] + bb;
-                    if (ACT) { z0 = tanhf(z0); z1 = tanhf(z1); }
-                    Y[uu * 32 + mt * 16 + g] = z0;
-                    Y[uu * 32 + mt * 16 + g + 8] = z1;
-                }
+        for (int mt = 0; mt < 2; mt++) {
+            const int r = mt * 16 + g;
+            float z00 = acc[mt][0] + bb0, z01 = acc[mt][1] + bb1;       // replica r
+            float z10 = acc[mt][2] + bb0, z11 = acc[mt][3] + bb1;       // replica r + 8
+            if (HIDDEN) {
+                uint32_t* Yp = static_cast<uint32_t*>(Y) + (u0 >> 1) * kActStride;
+                Yp[r] = pack_bf16x2(tanhf(z00), tanhf(z01));
+                Yp[r + 8] = pack_bf16x2(tanhf(z10), tanhf(z11));
+            } else {
+                float* Yf = static_cast<float*>(Y);
+                if (u0 < UNITS) { Yf[u0 * kOutStride + r] = z00; Yf[u0 * kOutStride + r + 8] = z10; }
+                if (u0 + 1 < UNITS) { Yf[(u0 + 1) * kOutStride + r] = z01; Yf[(u0 + 1) * kOutStride + r + 8] = z11; }
             }
         }
     }
 }
 
-// features feat[8][32] -> act1[64][32] -> act2[64][32] -> outs[26][32]; a
-// barrier after each layer (called by every thread of the CTA)
-__device__ __forceinline__ void mlp_block(const __nv_bfloat16* __restrict__ w, const float* feat, float* act1,
-                                          float* act2, float* outs, int warp, int W, int lane) {
-    mlp_layer_mma<kMlpIn, kMlpHidden, true>(w + kOffW1, w + kOffB1, feat, act1, warp, W, lane);
+// features (bufA rows 0..3) -> hidden 1 (bufB) -> hidden 2 (bufA) -> outputs
+// (bufB, FP32); a barrier after each layer (called by every thread of the CTA).
+// Each buffer is read only by the layer after the one that wrote it.
+__device__ __forceinline__ void mlp_block(const __nv_bfloat16* __restrict__ w, uint32_t* bufA, uint32_t* bufB,
+                                          int warp, int W, int lane) {
+    mlp_layer_mma<kMlpIn, kMlpHidden, true>(w + kOffW1, w + kOffB1, bufA, bufB, warp, W, lane);
     __syncthreads();
-    mlp_layer_mma<kMlpHidden, kMlpHidden, true>(w + kOffW2, w + kOffB2, act1, act2, warp, W, lane);
+    mlp_layer_mma<kMlpHidden, kMlpHidden, true>(w + kOffW2, w + kOffB2, bufB, bufA, warp, W, lane);
     __syncthreads();
-    mlp_layer_mma<kMlpHidden, kMlpOut, false>(w + kOffW3, w + kOffB3, act2, outs, warp, W, lane);
+    mlp_layer_mma<kMlpHidden, kMlpOut, false>(w + kOffW3, w + kOffB3, bufA, bufB, warp, W, lane);
     __syncthreads();
+}
+
+// the features of one replica into packed row pairs of bufA (lane = replica)
+__device__ __forceinline__ void store_features(uint32_t* bufA, const float* f, int lane) {
+#pragma unroll
+    for (int kp = 0; kp < kMlpIn / 2; kp++) bufA[kp * kActStride + lane] = pack_bf16x2(f[2 * kp], f[2 * kp + 1]);
 }
 
 __device__ __forceinline__ float argf(float2 a) { return atan2f(a.y, a.x); }
 
-// feat[8][32] + act1, act2 [64][32] + outs[26][32] floats, then the BF16 weights
-constexpr int kMlpSmemFloats = (kMlpIn + 2 * kMlpHidden + kMlpOut) * 32;
+// TMA chunks in flight per warp.  Two (one being read, one loading) keep the
+// kernel's shared memory under a third of the SM's, so three CTAs of 8 warps
+// share an SM (a chunk takes longer to read than to load from L2).
+constexpr int kLStages = 2;
+// two network buffers of 32 packed rows each (the outputs, 26 FP32 rows of
+// kOutStride, fit in one)
+constexpr int kMlpBufWords = (kMlpHidden / 2) * kActStride;
+static_assert(kMlpOut * kOutStride <= kMlpBufWords, "output rows fit a network buffer");
+
+// amplitudes [N+1][32] float2, partial fields [W][32] float4, TMA rings
+// [W][kLStages][kStage] int2, their barriers [W][kLStages], then the two
+// network buffers
+__host__ __device__ inline size_t learned_base_bytes(int N, int warps) {
+    return (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)warps * kRepBlock * sizeof(float4) +
+           (size_t)warps * kLStages * kStage * sizeof(int2) + (size_t)warps * kLStages * sizeof(uint64_t) +
+           (size_t)2 * kMlpBufWords * sizeof(uint32_t);
+}
 
 // cluster variant: the partial-field exchange buffer [2][C][32] float4 after
-// the weights, at a 16-byte boundary
+// the network buffers, at a 16-byte boundary
 __host__ __device__ inline size_t learned_cluster_buffer_offset(int N, int warps) {
-    return (sweep_smem_bytes(N, warps) + (size_t)kMlpSmemFloats * sizeof(float) +
-            (size_t)kMlpParams * sizeof(__nv_bfloat16) + 15) & ~(size_t)15;
+    return (learned_base_bytes(N, warps) + 15) & ~(size_t)15;
 }
 
 inline size_t learned_smem_bytes(int N, int warps, int C = 1) {
     if (C > 1) return learned_cluster_buffer_offset(N, warps) + (size_t)2 * C * kRepBlock * sizeof(float4);
-    return sweep_smem_bytes(N, warps) + (size_t)kMlpSmemFloats * sizeof(float) +
-           (size_t)kMlpParams * sizeof(__nv_bfloat16) + 16;
+    return learned_base_bytes(N, warps);
 }
 
 // CL: one replica block over a thread-block cluster of P.cluster CTAs.  Each
@@ -139,7 +170,7 @@ inline size_t learned_smem_bytes(int N, int warps, int C = 1) {
 // network and takes the same decision on the same numbers, so the amplitude
 // copies stay identical; rank 0 writes records, trace and results.
 template <bool CL>
-__global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams P, const LearnParams L) {
+__global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams P, const LearnParams L) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int C = CL ? P.cluster : 1;
     const uint32_t rank = CL ? cluster_rank() : 0u;
@@ -152,14 +183,12 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
     float2* sp = reinterpret_cast<float2*>(smem_raw);
     float4* red = reinterpret_cast<float4*>(sp + (size_t)(N + 1) * kRepBlock);
     int2* ring_all = reinterpret_cast<int2*>(red + (size_t)W * kRepBlock);
-    int2* ring = ring_all + (size_t)warp * kStages * kStage;
-    uint64_t* bars_all = reinterpret_cast<uint64_t*>(ring_all + (size_t)W * kStages * kStage);
-    uint64_t* bars = bars_all + warp * kStages;
-    float* feat = reinterpret_cast<float*>(bars_all + W * kStages);
-    float* act1 = feat + kMlpIn * 32;
-    float* act2 = act1 + kMlpHidden * 32;
-    float* outs = act2 + kMlpHidden * 32;
-    __nv_bfloat16* wsm = reinterpret_cast<__nv_bfloat16*>(outs + kMlpOut * 32);
+    int2* ring = ring_all + (size_t)warp * kLStages * kStage;
+    uint64_t* bars_all = reinterpret_cast<uint64_t*>(ring_all + (size_t)W * kLStages * kStage);
+    uint64_t* bars = bars_all + warp * kLStages;
+    uint32_t* bufA = reinterpret_cast<uint32_t*>(bars_all + W * kLStages);
+    uint32_t* bufB = bufA + kMlpBufWords;
+    const float* outs = reinterpret_cast<const float*>(bufB);
     float4* cred = CL ? reinterpret_cast<float4*>(smem_raw + learned_cluster_buffer_offset(N, W)) : nullptr;
 
     const bool active = lane < U.rep_count;
@@ -171,8 +200,6 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
         sp[idx] = v;
     }
     if (threadIdx.x < kRepBlock) sp[N * kRepBlock + threadIdx.x] = make_float2(1.f, 0.f);
-    if (learned)
-        for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) wsm[i] = L.w[i];
 
     double E = 0.0, beta_d = 0.0;
     float beta = 0.f;
@@ -201,7 +228,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
     st.part0 = gw * (kSplit / TW);
     st.part1 = (gw + 1) * (kSplit / TW);
     if (lane == 0) {
-        for (int s = 0; s < kStages; s++) mbar_init(bars + s, 1);
+        for (int s = 0; s < kLStages; s++) mbar_init(bars + s, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         fence_async_shared();
     }
@@ -211,7 +238,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
     bool ok_wait = true;
     auto issue = [&]() {
         if (pc.m >= total) return;
-        const uint32_t slot = issued % kStages;
+        const uint32_t slot = issued % kLStages;
         if (lane == 0) {
             const int64_t b = __ldg(P.chunk_start + pc.c), e = __ldg(P.chunk_start + pc.c + 1);
             const uint32_t bytes = (uint32_t)((e - b) * sizeof(int2));
@@ -221,7 +248,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
         issued++;
         st.next(pc);
     };
-    for (int s = 0; s < kStages; s++) issue();
+    for (int s = 0; s < kLStages; s++) issue();
     __syncthreads();
     if (CL) cluster_sync();                    // every CTA runs before the first remote store
     uint32_t xchg = 0;                         // exchanges so far (buffer parity)
@@ -233,8 +260,8 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
             int c, c_end;
             st.range(m, which, c, c_end);
             for (; c < c_end; c++) {
-                const uint32_t slot = consumed % kStages;
-                if (ok_wait) ok_wait = mbar_wait(bars + slot, (consumed / kStages) & 1u, P.status);
+                const uint32_t slot = consumed % kLStages;
+                if (ok_wait) ok_wait = mbar_wait(bars + slot, (consumed / kLStages) & 1u, P.status);
                 const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
                 const int k2 = 2 * (which & 1);
                 if (S.fc_tiles && which < 2) accumulate_tiles(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
@@ -295,14 +322,13 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
             if (learned) {
                 float f[kMlpIn];
                 pair_features(ai, aj, hi1, hj1, beta, f);
-#pragma unroll
-                for (int i = 0; i < kMlpIn; i++) feat[i * 32 + lane] = f[i];
+                store_features(bufA, f, lane);
             }
         }
         // ---- proposal -------------------------------------------------------------
         if (learned) {
             __syncthreads();
-            mlp_block(wsm, feat, act1, act2, outs, warp, W, lane);
+            mlp_block(L.w, bufA, bufB, warp, W, lane);
         }
         if (warp == 0) {
             if (!learned) {
@@ -315,7 +341,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
             } else {
                 float out[kMlpOut];
 #pragma unroll
-                for (int o = 0; o < kMlpOut; o++) out[o] = outs[o * 32 + lane];
+                for (int o = 0; o < kMlpOut; o++) out[o] = outs[o * kOutStride + lane];
                 ProposalParams pp;
                 decode_outputs(out, pp);
                 ok = sample_move(g, pp, tn, psi_i, psi_j);
@@ -355,13 +381,12 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
             if (learned) {
                 float f[kMlpIn];
                 pair_features(ain, ajn, hi2, hj2, beta, f);
-#pragma unroll
-                for (int i = 0; i < kMlpIn; i++) feat[i * 32 + lane] = f[i];
+                store_features(bufA, f, lane);
             }
         }
         if (learned) {
             __syncthreads();
-            mlp_block(wsm, feat, act1, act2, outs, warp, W, lane);
+            mlp_block(L.w, bufA, bufB, warp, W, lane);
         }
         if (warp == 0) {
             bool accept;
@@ -371,7 +396,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
             } else {
                 float out[kMlpOut];
 #pragma unroll
-                for (int o = 0; o < kMlpOut; o++) out[o] = outs[o * 32 + lane];
+                for (int o = 0; o < kMlpOut; o++) out[o] = outs[o * kOutStride + lane];
                 ProposalParams pr;
                 decode_outputs(out, pr);
                 // The sampler proposes t' only inside I = (1e-7, 1 - 1e-7), so the
@@ -424,7 +449,7 @@ __global__ void __launch_bounds__(256, 2) learned_sweep_kernel(const SweepParams
         __syncthreads();
     }
     if (!ok_wait && lane == 0)
-        for (uint32_t q = consumed; q < issued; q++) mbar_wait(bars + q % kStages, (q / kStages) & 1u, P.status);
+        for (uint32_t q = consumed; q < issued; q++) mbar_wait(bars + q % kLStages, (q / kLStages) & 1u, P.status);
     if (writer) {
         for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
             const int site = idx >> 5, l = idx & 31;
