@@ -144,12 +144,12 @@ constexpr int kMlpBufWords = (kMlpHidden / 2) * kActStride;
 static_assert(kMlpOut * kOutStride <= kMlpBufWords, "output rows fit a network buffer");
 
 // amplitudes [N+1][32] float2, partial fields [W][32] float4, TMA rings
-// [W][kLStages][kStage] int2, their barriers [W][kLStages], then the two
-// network buffers
+// [W][kLStages][kStage] int2, their barriers [W][kLStages], the two network
+// buffers, then the roles' exchange rows [kXchRows][32] float
 __host__ __device__ inline size_t learned_base_bytes(int N, int warps) {
     return (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)warps * kRepBlock * sizeof(float4) +
            (size_t)warps * kLStages * kStage * sizeof(int2) + (size_t)warps * kLStages * sizeof(uint64_t) +
-           (size_t)2 * kMlpBufWords * sizeof(uint32_t);
+           (size_t)2 * kMlpBufWords * sizeof(uint32_t) + (size_t)kXchRows * kRepBlock * sizeof(float);
 }
 
 // cluster variant: the partial-field exchange buffer [2][C][32] float4 after
@@ -189,6 +189,8 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
     uint32_t* bufA = reinterpret_cast<uint32_t*>(bars_all + W * kLStages);
     uint32_t* bufB = bufA + kMlpBufWords;
     const float* outs = reinterpret_cast<const float*>(bufB);
+    float* xch = reinterpret_cast<float*>(bufB + kMlpBufWords);
+    auto out_of = [&](int o) { return outs[o * kOutStride + lane]; };
     float4* cred = CL ? reinterpret_cast<float4*>(smem_raw + learned_cluster_buffer_offset(N, W)) : nullptr;
 
     const bool active = lane < U.rep_count;
@@ -205,13 +207,15 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
     float beta = 0.f;
     long long nacc = 0, nprop = 0;
     uint32_t k0 = 0, k1 = 0;
+    if (active) {                               // every warp may run a sampling role
+        const uint64_t key = P.key[gr];
+        k0 = (uint32_t)key;
+        k1 = (uint32_t)(key >> 32);
+    }
     if (warp == 0 && active) {
         E = P.energy[gr];
         beta_d = P.beta[gr];
         beta = (float)beta_d;
-        const uint64_t key = P.key[gr];
-        k0 = (uint32_t)key;
-        k1 = (uint32_t)(key >> 32);
     }
     const long long sweep0 = *P.sweep_counter;
     const int steps = N / 2, total = P.nsweeps * steps;
@@ -314,7 +318,7 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
         const float2 hi1 = make_float2(hs1.x, hs1.y), hj1 = make_float2(hs1.z, hs1.w);
         float cu = 0.f, lq_fwd = 0.f, lq_ratio = 0.f, tn = 0.5f, psi_i = 0.f, psi_j = 0.f, Ssum = 1.f;
         bool ok = true;
-        MoveStream g{k0, k1, (uint32_t)k, (uint32_t)sw, (uint32_t)((uint64_t)sw >> 32), 0u, 4u, U4{0, 0, 0, 0}};
+        MoveStream g = role_stream(k0, k1, (uint32_t)k, (uint64_t)sw, kAcceptBlock);   // accept and record draws
         if (warp == 0) {
             ai = sp[i0 * kRepBlock + lane];
             aj = sp[j0 * kRepBlock + lane];
@@ -329,6 +333,8 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
         if (learned) {
             __syncthreads();
             mlp_block(L.w, bufA, bufB, warp, W, lane);
+            for (int r = warp; r < kRoles; r += W) learned_role(r, true, out_of, xch, lane, k0, k1, (uint32_t)k, sw);
+            __syncthreads();
         }
         if (warp == 0) {
             if (!learned) {
@@ -339,20 +345,28 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
                 psi_i = argf(ain) + argf(hi1);
                 psi_j = argf(ajn) + argf(hj1);
             } else {
-                float out[kMlpOut];
-#pragma unroll
-                for (int o = 0; o < kMlpOut; o++) out[o] = outs[o * kOutStride + lane];
-                ProposalParams pp;
-                decode_outputs(out, pp);
-                ok = sample_move(g, pp, tn, psi_i, psi_j);
+                // the roles' draws: t' = X/(X+Y) inside (kTEdge, 1 - kTEdge) and
+                // both phases, else the move is rejected
+                const float X = xch[X_X * 32 + lane], Y = xch[X_Y * 32 + lane];
+                ok = X >= 0.f && Y >= 0.f && X + Y > 0.f && xch[X_OK0 * 32 + lane] != 0.f &&
+                     xch[X_OK1 * 32 + lane] != 0.f;
                 if (ok) {
+                    tn = X / (X + Y);
+                    ok = tn > kTEdge && tn < 1.0f - kTEdge;
+                }
+                if (ok) {
+                    psi_i = xch[X_PSI0 * 32 + lane];
+                    psi_j = xch[X_PSI1 * 32 + lane];
                     const float mi = sqrtf(Ssum * tn), mj = sqrtf(Ssum * (1.0f - tn));
                     float s1, c1, s2, c2;
                     sincosf(psi_i - argf(hi1), &s1, &c1);
                     sincosf(psi_j - argf(hj1), &s2, &c2);
                     ain = make_float2(mi * c1, mi * s1);
                     ajn = make_float2(mj * c2, mj * s2);
-                    lq_fwd = log_learned_density(pp, tn, psi_i, psi_j) - log_plain_density(tn);
+                    // log q_L(x'|x) = log Beta + both mixtures, as log_learned_density
+                    lq_fwd = log_beta_pdf_lg(tn, xch[X_A * 32 + lane], xch[X_B * 32 + lane], xch[X_LGA * 32 + lane],
+                                             xch[X_LGB * 32 + lane], xch[X_LGAB * 32 + lane]) +
+                             xch[X_VM0 * 32 + lane] + xch[X_VM1 * 32 + lane] - log_plain_density(tn);
                 } else {
                     ain = ai;
                     ajn = aj;
@@ -382,11 +396,16 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
                 float f[kMlpIn];
                 pair_features(ain, ajn, hi2, hj2, beta, f);
                 store_features(bufA, f, lane);
+                // the reverse move's phases, measured from the fields at x'
+                xch[X_PSI0 * 32 + lane] = argf(ai) + argf(hi2);
+                xch[X_PSI1 * 32 + lane] = argf(aj) + argf(hj2);
             }
         }
         if (learned) {
             __syncthreads();
             mlp_block(L.w, bufA, bufB, warp, W, lane);
+            for (int r = warp; r < kRoles; r += W) learned_role(r, false, out_of, xch, lane, k0, k1, (uint32_t)k, sw);
+            __syncthreads();
         }
         if (warp == 0) {
             bool accept;
@@ -394,11 +413,6 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
                 if (beta_d == 0.0) accept = true;
                 else accept = (dE <= 0.f) || (cu < expf(-beta * dE));
             } else {
-                float out[kMlpOut];
-#pragma unroll
-                for (int o = 0; o < kMlpOut; o++) out[o] = outs[o * kOutStride + lane];
-                ProposalParams pr;
-                decode_outputs(out, pr);
                 // The sampler proposes t' only inside I = (1e-7, 1 - 1e-7), so the
                 // move's density is q_L 1[t' in I]; the reverse move exists only
                 // if the current t is in I as well.  Accepting only then gives
@@ -407,8 +421,10 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
                 const float t = fmaf(ai.x, ai.x, ai.y * ai.y) / Ssum;
                 const bool t_in = t > kTEdge && t < 1.0f - kTEdge;
                 if (t_in) {
-                    const float lq_rev = log_learned_density(pr, t, argf(ai) + argf(hi2), argf(aj) + argf(hj2)) -
-                                         log_plain_density(t);
+                    const float lq_rev = log_beta_pdf_lg(t, xch[X_A * 32 + lane], xch[X_B * 32 + lane],
+                                                         xch[X_LGA * 32 + lane], xch[X_LGB * 32 + lane],
+                                                         xch[X_LGAB * 32 + lane]) +
+                                         xch[X_VM0 * 32 + lane] + xch[X_VM1 * 32 + lane] - log_plain_density(t);
                     lq_ratio = lq_rev - lq_fwd;
                 }
                 accept = ok && t_in && (logf(cu) < -beta * dE + lq_ratio);

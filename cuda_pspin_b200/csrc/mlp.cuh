@@ -82,32 +82,41 @@ struct ProposalParams {
     float w[2][4], mu[2][4], kappa[2][4];   // mixtures for psi_i, psi_j
 };
 
-__device__ __forceinline__ void decode_outputs(const float* o, ProposalParams& p) {
-    p.a = 0.05f + softplusf(o[0]);
-    p.b = 0.05f + softplusf(o[1]);
+__device__ __forceinline__ float decode_beta_param(float o) { return 0.05f + softplusf(o); }
+
+// one site's mixture from its 12 outputs q: softmax weights, means, kappas
+__device__ __forceinline__ void decode_site(const float* q, float* w, float* mu, float* kappa) {
+    float m = q[0];
     #pragma unroll
-    for (int s = 0; s < 2; s++) {
-        const float* q = o + 2 + 12 * s;
-        float m = q[0];
-        #pragma unroll
-        for (int k = 1; k < 4; k++) m = fmaxf(m, q[k]);
-        float z = 0.f;
-        #pragma unroll
-        for (int k = 0; k < 4; k++) { p.w[s][k] = expf(q[k] - m); z += p.w[s][k]; }
-        #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            p.w[s][k] /= z;
-            p.mu[s][k] = q[4 + k];
-            p.kappa[s][k] = kKappaMax * sigmoidf(q[8 + k]) + 0.01f;
-        }
+    for (int k = 1; k < 4; k++) m = fmaxf(m, q[k]);
+    float z = 0.f;
+    #pragma unroll
+    for (int k = 0; k < 4; k++) { w[k] = expf(q[k] - m); z += w[k]; }
+    #pragma unroll
+    for (int k = 0; k < 4; k++) {
+        w[k] /= z;
+        mu[k] = q[4 + k];
+        kappa[k] = kKappaMax * sigmoidf(q[8 + k]) + 0.01f;
     }
+}
+
+__device__ __forceinline__ void decode_outputs(const float* o, ProposalParams& p) {
+    p.a = decode_beta_param(o[0]);
+    p.b = decode_beta_param(o[1]);
+    #pragma unroll
+    for (int s = 0; s < 2; s++) decode_site(o + 2 + 12 * s, p.w[s], p.mu[s], p.kappa[s]);
 }
 
 // log I0(k) for 0 < k <= kKappaMax (CUDA's Bessel function, no overflow there)
 __device__ __forceinline__ float log_i0f(float k) { return logf(cyl_bessel_i0f(k)); }
 
+// log Beta(a,b) density at t with the log-gamma values given
+__device__ __forceinline__ float log_beta_pdf_lg(float t, float a, float b, float lga, float lgb, float lgab) {
+    return (a - 1.0f) * logf(t) + (b - 1.0f) * log1pf(-t) - (lga + lgb - lgab);
+}
+
 __device__ __forceinline__ float log_beta_pdf(float t, float a, float b) {
-    return (a - 1.0f) * logf(t) + (b - 1.0f) * log1pf(-t) - (lgammaf(a) + lgammaf(b) - lgammaf(a + b));
+    return log_beta_pdf_lg(t, a, b, lgammaf(a), lgammaf(b), lgammaf(a + b));
 }
 
 // log of the plain proposal density in (t', theta_i', theta_j'):
@@ -116,17 +125,21 @@ __device__ __forceinline__ float log_plain_density(float t) {
     return -0.5f * logf(t) - 0.5f * log1pf(-t) - 1.1447298858494002f - 2.0f * 1.8378770664093453f;
 }
 
-__device__ __forceinline__ float log_vm_mix(const ProposalParams& p, int s, float psi) {
+__device__ __forceinline__ float log_vm_mix_site(const float* w, const float* mu, const float* kappa, float psi) {
     float m = -1e30f, v[4];
     #pragma unroll
     for (int k = 0; k < 4; k++) {
-        v[k] = logf(p.w[s][k]) + p.kappa[s][k] * cosf(psi - p.mu[s][k]) - 1.8378770664093453f - log_i0f(p.kappa[s][k]);
+        v[k] = logf(w[k]) + kappa[k] * cosf(psi - mu[k]) - 1.8378770664093453f - log_i0f(kappa[k]);
         m = fmaxf(m, v[k]);
     }
     float z = 0.f;
     #pragma unroll
     for (int k = 0; k < 4; k++) z += expf(v[k] - m);
     return m + logf(z);
+}
+
+__device__ __forceinline__ float log_vm_mix(const ProposalParams& p, int s, float psi) {
+    return log_vm_mix_site(p.w[s], p.mu[s], p.kappa[s], psi);
 }
 
 __device__ __forceinline__ float log_learned_density(const ProposalParams& p, float t, float psi_i, float psi_j) {
@@ -195,6 +208,79 @@ __device__ __forceinline__ float vonmises_sample(MoveStream& g, float kappa) {
     return -10.0f;
 }
 
+// component k of a 4-component mixture for a uniform u by an unrolled scan
+// (constant indices keep the parameters in registers); returns its kappa, mu
+__device__ __forceinline__ void pick_component(const float* w, const float* mu, const float* kappa, float u,
+                                               float& kap, float& m) {
+    float acc = w[0];
+    kap = kappa[0];
+    m = mu[0];
+    bool done = u <= acc;
+#pragma unroll
+    for (int k = 1; k < 4; k++) {
+        if (!done) { kap = kappa[k]; m = mu[k]; }
+        acc += w[k];
+        done = done || u <= acc;
+    }
+}
+
+// ---- the learned move split in five independent roles ----------------------
+// Given the network outputs, the move's four random parts are independent:
+// t' = X/(X+Y) with X ~ Gamma(a), Y ~ Gamma(b), and each site's phase from
+// its own mixture.  Each role runs one of them as a complete rejection
+// sampler on its own sub-stream of the replica's move stream (Philox blocks
+// kRoleBlocks*r ..), so the roles can run on different warps at once and the
+// draw is still exact; the density's parts (log-gamma values, each site's
+// mixture log-density at its phase) go with them.  Role 4 takes lgamma(a+b).
+// Results go to rows of a [kXchRows][32] exchange buffer (lane = replica).
+constexpr int kRoles = 5;
+constexpr uint32_t kRoleBlocks = 40;               // >= 25 blocks a bounded gamma or von Mises draw can use
+constexpr uint32_t kAcceptBlock = kRoles * kRoleBlocks;   // the accept (and record) draws
+enum : int { X_A, X_B, X_X, X_Y, X_LGA, X_LGB, X_LGAB, X_PSI0, X_PSI1, X_VM0, X_VM1, X_OK0, X_OK1, kXchRows };
+
+__device__ __forceinline__ MoveStream role_stream(uint32_t k0, uint32_t k1, uint32_t step, uint64_t sw,
+                                                  uint32_t first_block) {
+    return MoveStream{k0, k1, step, (uint32_t)sw, (uint32_t)(sw >> 32), first_block, 4u, U4{0u, 0u, 0u, 0u}};
+}
+
+// out(o) reads output o of this lane's replica.  sample: forward move (draw
+// and density parts); otherwise the reverse density's parts at the phases
+// already in rows X_PSI0 / X_PSI1.
+template <class Out>
+__device__ __forceinline__ void learned_role(int r, bool sample, Out out, float* xch, int lane, uint32_t k0,
+                                             uint32_t k1, uint32_t step, uint64_t sw) {
+    if (r < 2) {
+        const float a = decode_beta_param(out(r));
+        xch[(X_A + r) * 32 + lane] = a;
+        xch[(X_LGA + r) * 32 + lane] = lgammaf(a);
+        if (sample) {
+            MoveStream g = role_stream(k0, k1, step, sw, kRoleBlocks * (uint32_t)r);
+            xch[(X_X + r) * 32 + lane] = gamma_sample(g, a);
+        }
+    } else if (r < 4) {
+        const int s = r - 2;
+        float q[12], w[4], mu[4], kap[4];
+#pragma unroll
+        for (int o = 0; o < 12; o++) q[o] = out(2 + 12 * s + o);
+        decode_site(q, w, mu, kap);
+        float psi = sample ? 0.0f : xch[(X_PSI0 + s) * 32 + lane];
+        bool ok = true;
+        if (sample) {
+            MoveStream g = role_stream(k0, k1, step, sw, kRoleBlocks * (uint32_t)r);
+            float kk, mm;
+            pick_component(w, mu, kap, g.uniform(), kk, mm);
+            const float v = vonmises_sample(g, kk);
+            ok = v >= -9.0f;
+            psi = mm + v;
+            xch[(X_PSI0 + s) * 32 + lane] = psi;
+            xch[(X_OK0 + s) * 32 + lane] = ok ? 1.0f : 0.0f;
+        }
+        xch[(X_VM0 + s) * 32 + lane] = ok ? log_vm_mix_site(w, mu, kap, psi) : 0.0f;
+    } else {
+        xch[X_LGAB * 32 + lane] = lgammaf(decode_beta_param(out(0)) + decode_beta_param(out(1)));
+    }
+}
+
 // returns false when a bounded sampler ran out (the move is then rejected)
 __device__ __forceinline__ bool sample_move(MoveStream& g, const ProposalParams& p, float& t, float& psi_i,
                                             float& psi_j) {
@@ -205,17 +291,8 @@ __device__ __forceinline__ bool sample_move(MoveStream& g, const ProposalParams&
     float psi[2];
 #pragma unroll
     for (int s = 0; s < 2; s++) {
-        // component choice by an unrolled scan (constant indices keep the
-        // parameters in registers)
-        const float u = g.uniform();
-        float acc = p.w[s][0], kap = p.kappa[s][0], mu = p.mu[s][0];
-        bool done = u <= acc;
-#pragma unroll
-        for (int k = 1; k < 4; k++) {
-            if (!done) { kap = p.kappa[s][k]; mu = p.mu[s][k]; }
-            acc += p.w[s][k];
-            done = done || u <= acc;
-        }
+        float kap, mu;
+        pick_component(p.w[s], p.mu[s], p.kappa[s], g.uniform(), kap, mu);
         const float v = vonmises_sample(g, kap);
         if (v < -9.0f) return false;
         psi[s] = mu + v;
