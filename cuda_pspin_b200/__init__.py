@@ -126,6 +126,8 @@ def load_library() -> ctypes.CDLL:
         "pspin_pt_shape": (ctypes.c_int, [vp, vp, vp, vp]),
         "pspin_overlap_counts": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int,
                                                 ctypes.c_double, ctypes.c_double, vp]),
+        "pspin_ifo_counts": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int,
+                                            ctypes.c_double, ctypes.c_double, vp, vp, vp, vp]),
         "pspin_exchange_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp,
                                                vp]),
         "pspin_checkpoint_load": (ctypes.c_int, [vp, ctypes.c_char_p]),

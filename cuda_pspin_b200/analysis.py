@@ -1,12 +1,18 @@
-"""Parisi overlap distribution P(q) of a set of PT runs, computed on the GPU.
+"""Overlap distributions of a set of PT runs, computed on the GPU.
 
 Reads the runs' configs.bin files (the engine's or the reference's drivers
-write the same format), histograms q_ab = Re sum_k a_k^a conj(a_k^b) / N over
-every saved configuration and replica pair at each temperature with
-`pspin_overlap_counts` (binned exactly as the reference bins), normalises
-each sample's histogram to a density and writes parisi_overlap.dat with the
-sample mean and jackknife error in the reference's format
-(analysis_pt.cpp:1337-1480):
+write the same format) and histograms, at each temperature and binned
+exactly as the reference bins:
+  * the Parisi overlap q_ab = Re sum_k a_k^a conj(a_k^b) / N over every saved
+    configuration and replica pair (`pspin_overlap_counts`;
+    analysis_pt.cpp:1337-1480 -> parisi_overlap.dat);
+  * the intensity fluctuation overlap C_ab of I_k = |a_k|^2 about each
+    replica's time average, per configuration and pair, and the
+    experimental IFO of the time-averaged spectra, once per pair
+    (`pspin_ifo_counts`; analysis_pt.cpp:1498-1663 -> ifo_overlap.dat,
+    :1679-1850 -> exp_ifo_overlap.dat).
+Each sample's histogram is normalised to a density and the files hold the
+sample mean and jackknife error in the reference's format:
 
     python -m cuda_pspin_b200.analysis -N 12 -NT 4 -nrep 2 [-nbins 100] [--data data] [--out analysis_gpu]
 """
@@ -73,17 +79,52 @@ def overlap_histograms(cfg: np.ndarray, nbins: int = 100, qmin: float = -1.0, qm
     return counts / (n_overlaps * dq) if n_overlaps > 0 else counts.astype(np.float64)
 
 
+def ifo_histograms(cfg: np.ndarray, nbins: int = 100, cmin: float = -1.0,
+                   cmax: float = 1.0) -> tuple[np.ndarray, np.ndarray]:
+    """IFO and experimental-IFO densities [NT, nbins] of one sample: counts /
+    (overlaps counted * dC), zero where none was counted, as the reference
+    normalises."""
+    nsnap, NT, nrep, N, _ = cfg.shape
+    ic, inn = np.zeros((NT, nbins), np.int64), np.zeros(NT, np.int64)
+    ec, en = np.zeros((NT, nbins), np.int64), np.zeros(NT, np.int64)
+    c = np.ascontiguousarray(cfg, np.float64)
+    _check(load_library().pspin_ifo_counts(N, NT, nrep, nsnap, _ptr(c), nbins, cmin, cmax, _ptr(ic), _ptr(inn),
+                                           _ptr(ec), _ptr(en)))
+    dc = (cmax - cmin) / nbins
+
+    def dens(counts, n):
+        out = counts.astype(np.float64)
+        for t in range(NT):
+            if n[t] > 0:
+                out[t] /= (n[t] * dc)
+        return out
+    return dens(ic, inn), dens(ec, en)
+
+
+PARISI_HEADER = ["# Parisi overlap distribution P(q)", "# N={N} NT={NT} nrep={nrep} nbins={nbins} nsamples={S}",
+                 "# q = Re[ (1/N) sum_i a_i^alpha * conj(a_i^beta) ]", "# Columns: q_center  P(q)  Error_jk  Temperature",
+                 "# NT blocks separated by blank lines"]
+IFO_HEADER = ["# Intensity Fluctuation Overlap (IFO) distribution P(C)",
+              "# N={N} NT={NT} nrep={nrep} nbins={nbins} nsamples={S}",
+              "# C^{{ab}} = sum_k delta_k^a delta_k^b / sqrt(sum_k (delta_k^a)^2 * sum_k (delta_k^b)^2)",
+              "# delta_k^r = I_k^r - <I_k^r>_sweeps,  I_k = |a_k|^2", "# Columns: C_center  P(C)  Error_jk  Temperature",
+              "# NT blocks separated by blank lines"]
+EXP_IFO_HEADER = ["# Experimental IFO distribution P(C)", "# N={N} NT={NT} nrep={nrep} nbins={nbins} nsamples={S}",
+                  "# delta_k^r = <I_k>_r - <<I_k>>,  <<I_k>> = (1/R) sum_r <I_k>_r",
+                  "# C^{{ab}} = sum_k d_k^a d_k^b / sqrt(sum_k (d_k^a)^2 * sum_k (d_k^b)^2)",
+                  "# Columns: C_center  P(C)  Error_jk  Temperature", "# NT blocks separated by blank lines"]
+
+
 def write_parisi_overlap(path: str, hists: np.ndarray, temps, N: int, NT: int, nrep: int, nbins: int,
-                         qmin: float = -1.0, qmax: float = 1.0) -> None:
-    """hists [nsamples, NT, nbins]; the sample mean and jackknife error per bin."""
+                         qmin: float = -1.0, qmax: float = 1.0, header=PARISI_HEADER) -> None:
+    """hists [nsamples, NT, nbins]; the sample mean and jackknife error per bin
+    under the given header lines (the P(q), IFO and experimental-IFO files
+    share this layout)."""
     S = hists.shape[0]
     dq = (qmax - qmin) / nbins
     with open(path, "w") as f:
-        f.write("# Parisi overlap distribution P(q)\n")
-        f.write(f"# N={N} NT={NT} nrep={nrep} nbins={nbins} nsamples={S}\n")
-        f.write("# q = Re[ (1/N) sum_i a_i^alpha * conj(a_i^beta) ]\n")
-        f.write("# Columns: q_center  P(q)  Error_jk  Temperature\n")
-        f.write("# NT blocks separated by blank lines\n")
+        for line in header:
+            f.write(line.format(N=N, NT=NT, nrep=nrep, nbins=nbins, S=S) + "\n")
         for ti in range(hists.shape[1]):
             f.write("\n")
             for b in range(nbins):
@@ -118,12 +159,20 @@ def main(argv=None) -> int:
     if not runs:
         print("no runs with N=%d NT=%d nrep=%d under %s" % (a.N, a.NT, a.nrep, a.data), file=sys.stderr)
         return 1
-    hists = np.stack([overlap_histograms(read_configs(d, a.N, a.NT, a.nrep), a.nbins) for _, d in runs])
+    hists, ifo, exp_ifo = [], [], []
+    for _, d in runs:
+        cfg = read_configs(d, a.N, a.NT, a.nrep)
+        hists.append(overlap_histograms(cfg, a.nbins))
+        i, e = ifo_histograms(cfg, a.nbins)
+        ifo.append(i)
+        exp_ifo.append(e)
     temps = temperatures(runs[0][1], a.NT)
     os.makedirs(a.out, exist_ok=True)
-    path = os.path.join(a.out, "parisi_overlap.dat")
-    write_parisi_overlap(path, hists, temps, a.N, a.NT, a.nrep, a.nbins)
-    print("%d samples, written %s" % (len(runs), path))
+    for name, h, header in (("parisi_overlap.dat", hists, PARISI_HEADER), ("ifo_overlap.dat", ifo, IFO_HEADER),
+                            ("exp_ifo_overlap.dat", exp_ifo, EXP_IFO_HEADER)):
+        path = os.path.join(a.out, name)
+        write_parisi_overlap(path, np.stack(h), temps, a.N, a.NT, a.nrep, a.nbins, header=header)
+        print("%d samples, written %s" % (len(runs), path))
     return 0
 
 

@@ -1597,6 +1597,23 @@ extern "C" int pspin_overlap_counts(int N, int NT, int nrep, int nsnap, const do
     return PSPIN_OK;
 }
 
+extern "C" int pspin_ifo_counts_impl(int N, int NT, int nrep, int nsnap, const double* configs, int nbins,
+                                     double cmin, double cmax, long long* ifo_counts, long long* ifo_n,
+                                     long long* exp_counts, long long* exp_n, const char** err);
+
+extern "C" int pspin_ifo_counts(int N, int NT, int nrep, int nsnap, const double* configs, int nbins, double cmin,
+                                double cmax, int64_t* ifo_counts, int64_t* ifo_n, int64_t* exp_counts,
+                                int64_t* exp_n) {
+    const char* err = nullptr;
+    const int rc = pspin_ifo_counts_impl(N, NT, nrep, nsnap, configs, nbins, cmin, cmax,
+                                         reinterpret_cast<long long*>(ifo_counts), reinterpret_cast<long long*>(ifo_n),
+                                         reinterpret_cast<long long*>(exp_counts), reinterpret_cast<long long*>(exp_n),
+                                         &err);
+    if (rc == 1) return fail(PSPIN_ERR_ARG, "%s", err);
+    if (rc) return fail(PSPIN_ERR_CUDA, "IFO counts: %s", err);
+    return PSPIN_OK;
+}
+
 extern "C" int pspin_exchange_host(int n_samples, int NT, int nrep, const double* beta_sched, const double* energy,
                                    const int64_t* rep_off, int32_t* perm, uint64_t* drand_state, int64_t* ex_acc,
                                    int64_t* ex_prop, double* betas) {

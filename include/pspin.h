@@ -187,6 +187,17 @@ int  pspin_exchange_host(int n_samples, int NT, int nrep, const double* beta_sch
  * the same bins). */
 int  pspin_overlap_counts(int N, int NT, int nrep, int nsnap, const double* configs, int nbins, double qmin,
                           double qmax, int64_t* counts);
+/* Intensity fluctuation overlap histograms of one sample on the GPU (the IFO
+ * loop of analysis_pt.cpp:1498-1619 and the experimental IFO of
+ * :1679-1806), same configs layout: with I_k = |a_k|^2 and <I_k>_r its mean
+ * over the snapshots, IFO bins C_ab = sum_k d_a d_b / sqrt(sum d_a^2 sum
+ * d_b^2) of d = I_k - <I_k>_r per snapshot and pair, the experimental IFO
+ * the same of d = <I_k>_r - (replica mean of <I_k>_r) once per pair.
+ * ifo_counts / exp_counts [NT][nbins], ifo_n / exp_n [NT] the overlaps
+ * counted (pairs with a zero norm are skipped, as the reference skips them);
+ * either pair of outputs may be NULL.  Binned as the reference bins. */
+int  pspin_ifo_counts(int N, int NT, int nrep, int nsnap, const double* configs, int nbins, double cmin,
+                      double cmax, int64_t* ifo_counts, int64_t* ifo_n, int64_t* exp_counts, int64_t* exp_n);
 /* NT, replicas per temperature and exchange period set by pspin_pt_init (0s before). */
 int  pspin_pt_shape(pspin_state* s, int* NT, int* nrep_per_temp, int* pt_freq);
 /* Block-shape autotuner (no reference counterpart): times `sweeps` sweeps

@@ -1,9 +1,13 @@
-"""Host parts of the GPU P(q) analysis: configs.bin and energy_accept.txt
-reading, run discovery, and the jackknife / file format of
-parisi_overlap.dat (analysis_pt.cpp:1418-1480), on synthetic files."""
+"""Host parts of the GPU overlap analyses: configs.bin and energy_accept.txt
+reading, run discovery, the jackknife / file format of parisi_overlap.dat
+(analysis_pt.cpp:1418-1480), and the IFO arithmetic order checked against
+the reference analysis_pt, on synthetic files."""
+import math
 import os
+import subprocess
 
 import numpy as np
+import pytest
 
 from cuda_pspin_b200 import analysis as A
 
@@ -53,3 +57,118 @@ def test_jackknife_file(tmp_path):
     np.testing.assert_allclose(rows[:, 2], err.ravel(), rtol=1e-8)
     np.testing.assert_allclose(rows[:nbins, 0], -1 + (np.arange(nbins) + 0.5) * 0.2, atol=1e-12)
     assert set(rows[:nbins, 3]) == {1.2} and set(rows[nbins:, 3]) == {0.4}
+
+
+# ---- IFO / experimental IFO: restatement of the reference's FP64 order ------
+def _intensity(x, k):
+    return x[k, 0] * x[k, 0] + x[k, 1] * x[k, 1]
+
+
+def _ifo_restated(cfg, nbins):
+    """Plain-Python (round-to-nearest doubles, no contraction) restatement of
+    analysis_pt.cpp:1547-1607 (IFO) and :1745-1793 (experimental IFO) in the
+    operation order pspin_ifo_counts uses: densities [NT, nbins] of each."""
+    nsnap, NT, nrep, N, _ = cfg.shape
+    cmin, dc = -1.0, 2.0 / nbins
+    ifo, ex = np.zeros((NT, nbins)), np.zeros((NT, nbins))
+
+    def add(cnt, num, den):
+        if den <= 0:
+            return 0
+        cnt[min(max(int((num / den - cmin) / dc), 0), nbins - 1)] += 1
+        return 1
+    for t in range(NT):
+        mean = []
+        for r in range(nrep):
+            row = []
+            for k in range(N):
+                s = 0.0
+                for sn in range(nsnap):
+                    s = s + _intensity(cfg[sn, t, r], k)
+                row.append(s / nsnap)
+            mean.append(row)
+        cnt, n = [0] * nbins, 0
+        for sn in range(nsnap):
+            d = [[_intensity(cfg[sn, t, r], k) - mean[r][k] for k in range(N)] for r in range(nrep)]
+            n2 = []
+            for r in range(nrep):
+                s = 0.0
+                for k in range(N):
+                    s = s + d[r][k] * d[r][k]
+                n2.append(s)
+            for a in range(nrep):
+                for b in range(a + 1, nrep):
+                    num = 0.0
+                    for k in range(N):
+                        num = num + d[a][k] * d[b][k]
+                    n += add(cnt, num, math.sqrt(n2[a] * n2[b]))
+        if n:
+            ifo[t] = np.array(cnt) / (n * dc)
+        g = []
+        for k in range(N):
+            s = 0.0
+            for r in range(nrep):
+                s = s + mean[r][k]
+            g.append(s / nrep)
+        d = [[mean[r][k] - g[k] for k in range(N)] for r in range(nrep)]
+        cnt, n = [0] * nbins, 0
+        for a in range(nrep):
+            for b in range(a + 1, nrep):
+                na = nb = num = 0.0
+                for k in range(N):
+                    na = na + d[a][k] * d[a][k]
+                    nb = nb + d[b][k] * d[b][k]
+                    num = num + d[a][k] * d[b][k]
+                n += add(cnt, num, math.sqrt(na * nb))
+        if n:
+            ex[t] = np.array(cnt) / (n * dc)
+    return ifo, ex
+
+
+REF_ANALYSIS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                            "analysis_pt")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_ANALYSIS), reason="reference analysis_pt not built")
+def test_ifo_restatement_matches_analysis_pt(tmp_path):
+    """The operation order of pspin_ifo_counts, restated on the CPU, gives
+    ifo_overlap.dat and exp_ifo_overlap.dat identical to the reference
+    analysis_pt's on synthetic runs, including an overlap of exactly 1 (two
+    identical replicas: the last bin) and a replica with no fluctuation (zero
+    norm: skipped and not counted)."""
+    N, NT, nrep, nsnap, S, nbins = 6, 3, 3, 5, 4, 20
+    rng = np.random.default_rng(5)
+    cfgs = []
+    for s in range(S):
+        d = tmp_path / "data" / f"PT_N{N}_a0.5_Rinf_a00.5_NT{NT}_NR{nrep}_S{s}"
+        cfg = _fake_run(str(d), N, NT, nrep, nsnap, rng, s)
+        if s == 1:
+            cfg[:, 0, 2] = cfg[:, 0, 1]
+            cfg[:, 1, 0] = cfg[0, 1, 0]
+            with open(d / "configs.bin", "wb") as f:
+                np.array([N, NT, nrep], np.int32).tofile(f)
+                for k in range(nsnap):
+                    np.array([1000 + 10 * k], np.int32).tofile(f)
+                    cfg[k].tofile(f)
+        with open(d / "energy_accept.txt", "w") as f:           # nrep (E, acc) columns
+            f.write("# sweep\tTidx\tT" + "".join(f"\tE{r}/N\tacc{r}" for r in range(nrep)) + "\n")
+            for sw in range(3):
+                for t in range(NT):
+                    f.write("%d\t%d\t%.8f" % (sw, t, 1.5 - 0.25 * t) + "\t-1.00000000\t0.50000" * nrep + "\n")
+        with open(d / "exchanges.txt", "w") as f:
+            f.write("# sweep\tTidx\tT_high\tT_low\tn_acc\tn_prop\trate\n")
+            for sw in range(3):
+                for t in range(NT - 1):
+                    f.write("%d\t%d\t%.8f\t%.8f\t1\t2\t0.50000\n" % (sw, t, 1.5 - 0.25 * t, 1.25 - 0.25 * t))
+        cfgs.append(cfg)
+    p = subprocess.run([REF_ANALYSIS, "-N", str(N), "-NT", str(NT), "-nrep", str(nrep), "-nbins", str(nbins)],
+                       cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr[-1000:]
+    res = [_ifo_restated(c, nbins) for c in cfgs]
+    temps = A.temperatures(str(tmp_path / "data" / f"PT_N{N}_a0.5_Rinf_a00.5_NT{NT}_NR{nrep}_S0"), NT)
+    for i, (name, header) in enumerate((("ifo_overlap.dat", A.IFO_HEADER), ("exp_ifo_overlap.dat", A.EXP_IFO_HEADER))):
+        ours = tmp_path / ("ours_" + name)
+        A.write_parisi_overlap(str(ours), np.stack([r[i] for r in res]), temps, N, NT, nrep, nbins, header=header)
+        refs = [os.path.join(r, f) for r, _, fs in os.walk(tmp_path / "analysis") for f in fs if f == name]
+        assert len(refs) == 1
+        assert open(ours).read() == open(refs[0]).read(), name

@@ -115,33 +115,38 @@ def test_mc_driver_matches_reference_files(tmp_path):
 
 
 def test_gpu_overlap_distribution_matches_analysis_pt(tmp_path):
-    """P(q) from the saved configurations on the GPU (pspin_overlap_counts +
-    cuda_pspin_b200.analysis) equals the reference analysis_pt's
-    parisi_overlap.dat on the same runs: same bins, densities and jackknife
-    errors, same temperatures."""
+    """P(q), the IFO P(C) and the experimental-IFO P(C) from the saved
+    configurations on the GPU (pspin_overlap_counts, pspin_ifo_counts +
+    cuda_pspin_b200.analysis) equal the reference analysis_pt's
+    parisi_overlap.dat, ifo_overlap.dat and exp_ifo_overlap.dat on the same
+    runs: same headers, bins, densities and jackknife errors, same
+    temperatures."""
     flags = ["-N", "12", "-Tmax", "1.6", "-Tmin", "0.3", "-NT", "4", "-log_temp", "-nrep", "3", "-iter", "512",
              "-pt_freq", "1", "-save_freq", "8", "-seed", "11", "-label", "0", "-batch", "6"]
     run([os.path.join(BIN, "pspin_pt"), *flags], tmp_path)
     run([os.path.join(REF, "analysis_pt"), "-N", "12", "-NT", "4", "-nrep", "3", "--log-temp"], tmp_path)
-    refs = [os.path.join(r, f) for r, _, fs in os.walk(tmp_path / "analysis") for f in fs if f == "parisi_overlap.dat"]
-    assert len(refs) == 1
     p = subprocess.run([sys.executable, "-m", "cuda_pspin_b200.analysis", "-N", "12", "-NT", "4", "-nrep", "3",
                         "--out", str(tmp_path / "gpu")], cwd=tmp_path, capture_output=True, text=True, timeout=300,
                        env={**os.environ, "PYTHONPATH": ROOT})
     assert p.returncode == 0, p.stderr[-2000:]
-    ours = open(tmp_path / "gpu" / "parisi_overlap.dat").read().splitlines()
-    theirs = open(refs[0]).read().splitlines()
-    assert len(ours) == len(theirs)
-    n_rows = 0
-    for a, b in zip(ours, theirs):
-        if a.startswith("#") or not a.strip():
-            assert a == b
-            continue
-        x, y = np.array(a.split(), float), np.array(b.split(), float)
-        assert x[0] == y[0] and x[3] == y[3]
-        assert abs(x[1] - y[1]) <= 1e-12 * max(1.0, abs(y[1])) and abs(x[2] - y[2]) <= 1e-9 * max(1.0, abs(y[2]))
-        n_rows += 1
-    assert n_rows == 4 * 100
+    for name in ("parisi_overlap.dat", "ifo_overlap.dat", "exp_ifo_overlap.dat"):
+        refs = [os.path.join(r, f) for r, _, fs in os.walk(tmp_path / "analysis") for f in fs if f == name]
+        assert len(refs) == 1, name
+        ours = open(tmp_path / "gpu" / name).read().splitlines()
+        theirs = open(refs[0]).read().splitlines()
+        assert len(ours) == len(theirs), name
+        n_rows = filled = 0
+        for a, b in zip(ours, theirs):
+            if a.startswith("#") or not a.strip():
+                assert a == b, name
+                continue
+            x, y = np.array(a.split(), float), np.array(b.split(), float)
+            assert x[0] == y[0] and x[3] == y[3], name
+            assert abs(x[1] - y[1]) <= 1e-12 * max(1.0, abs(y[1])), (name, a, b)
+            assert abs(x[2] - y[2]) <= 1e-9 * max(1.0, abs(y[2])), (name, a, b)
+            n_rows += 1
+            filled += y[1] > 0
+        assert n_rows == 4 * 100 and filled > 4, name
 
 
 SA_FLAGS = ["-N", "12", "-nrep", "3", "-Tmax", "1.6", "-Tmin", "0.3", "-ntemp", "5", "-iter", "6", "-save_freq", "16",
