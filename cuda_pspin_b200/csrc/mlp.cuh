@@ -281,27 +281,6 @@ __device__ __forceinline__ void learned_role(int r, bool sample, Out out, float*
     }
 }
 
-// returns false when a bounded sampler ran out (the move is then rejected)
-__device__ __forceinline__ bool sample_move(MoveStream& g, const ProposalParams& p, float& t, float& psi_i,
-                                            float& psi_j) {
-    const float x = gamma_sample(g, p.a), y = gamma_sample(g, p.b);
-    if (x < 0.f || y < 0.f || x + y <= 0.f) return false;
-    t = x / (x + y);
-    if (!(t > kTEdge && t < 1.0f - kTEdge)) return false;
-    float psi[2];
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-        float kap, mu;
-        pick_component(p.w[s], p.mu[s], p.kappa[s], g.uniform(), kap, mu);
-        const float v = vonmises_sample(g, kap);
-        if (v < -9.0f) return false;
-        psi[s] = mu + v;
-    }
-    psi_i = psi[0];
-    psi_j = psi[1];
-    return true;
-}
-
 // ------------------------------------------------------------------ training
 // digamma by recurrence to x >= 6 and the asymptotic series
 // (Abramowitz & Stegun 6.3.18)
