@@ -12,13 +12,21 @@ exactly as the reference bins:
     (`pspin_ifo_counts`; analysis_pt.cpp:1498-1663 -> ifo_overlap.dat,
     :1679-1850 -> exp_ifo_overlap.dat).
 Each sample's histogram is normalised to a density and the files hold the
-sample mean and jackknife error in the reference's format:
+sample mean and jackknife error in the reference's format; from the same
+histograms, as analysis_pt does for each distribution (tags parisi, ifo,
+exp_ifo): {tag}_moments.dat (mean, variance, skewness, excess kurtosis with
+jackknife errors, analysis_pt.cpp:61-126), {tag}_glass_observables.dat (chi
+= N<x^2>, Binder g4, non-self-averaging A) and {tag}_sample_x2.dat
+(:209-305).  The host arithmetic follows the reference's operation order in
+IEEE doubles, so the printed numbers are the reference's (a single sample
+gives its -nan jackknife errors):
 
     python -m cuda_pspin_b200.analysis -N 12 -NT 4 -nrep 2 [-nbins 100] [--data data] [--out analysis_gpu]
 """
 from __future__ import annotations
 
 import argparse
+import math
 import os
 import re
 import sys
@@ -115,11 +123,41 @@ EXP_IFO_HEADER = ["# Experimental IFO distribution P(C)", "# N={N} NT={NT} nrep=
                   "# Columns: C_center  P(C)  Error_jk  Temperature", "# NT blocks separated by blank lines"]
 
 
+# ---- host arithmetic in the reference's order (IEEE doubles, x86 results) ---
+def _div(a, b):
+    """a / b with C's result for b == 0 (inf, or the negative default NaN)."""
+    if b == 0:
+        with np.errstate(all="ignore"):
+            return float(np.float64(a) / np.float64(b))
+    return a / b
+
+
+def _e(x) -> str:
+    """printf("%.8e") as glibc prints it (a NaN with its sign)."""
+    if math.isnan(x):
+        return "-nan" if math.copysign(1.0, x) < 0 else "nan"
+    return "%.8e" % x
+
+
+def _mean_rows(h: np.ndarray, skip: int = -1) -> np.ndarray:
+    """Per-bin sum over the samples s != skip in sample order, divided by
+    their count: h [S, nbins] (vectorised over bins only)."""
+    acc = np.zeros(h.shape[1])
+    n = 0
+    for s in range(h.shape[0]):
+        if s != skip:
+            acc = acc + h[s]
+            n += 1
+    with np.errstate(all="ignore"):
+        return acc / np.float64(n)
+
+
 def write_parisi_overlap(path: str, hists: np.ndarray, temps, N: int, NT: int, nrep: int, nbins: int,
                          qmin: float = -1.0, qmax: float = 1.0, header=PARISI_HEADER) -> None:
     """hists [nsamples, NT, nbins]; the sample mean and jackknife error per bin
     under the given header lines (the P(q), IFO and experimental-IFO files
-    share this layout)."""
+    share this layout; analysis_pt.cpp:1452-1477)."""
+    hists = np.asarray(hists, np.float64)
     S = hists.shape[0]
     dq = (qmax - qmin) / nbins
     with open(path, "w") as f:
@@ -127,23 +165,156 @@ def write_parisi_overlap(path: str, hists: np.ndarray, temps, N: int, NT: int, n
             f.write(line.format(N=N, NT=NT, nrep=nrep, nbins=nbins, S=S) + "\n")
         for ti in range(hists.shape[1]):
             f.write("\n")
+            h = hists[:, ti, :]
+            fP = _mean_rows(h)
+            jP = np.zeros(nbins)
+            for j in range(S):
+                lP = _mean_rows(h, j)
+                jP = jP + (lP - fP) * (lP - fP)
+            with np.errstate(all="ignore"):
+                jP = np.sqrt((S - 1.0) / S * jP)
             for b in range(nbins):
                 qc = qmin + (b + 0.5) * dq
-                col = [float(hists[s, ti, b]) for s in range(S)]
-                fP = 0.0
-                for v in col:
-                    fP += v
-                fP /= S
-                jP = 0.0
-                for j in range(S):
-                    lP = 0.0
-                    for s in range(S):
-                        if s != j:
-                            lP += col[s]
-                    lP /= (S - 1)
-                    jP += (lP - fP) * (lP - fP)
-                jP = np.sqrt((S - 1.0) / S * jP)
-                f.write("%.12f\t%.8e\t%.8e\t%.8f\n" % (qc, fP, jP, temps[ti]))
+                f.write("%.12f\t%s\t%s\t%.8f\n" % (qc, _e(float(fP[b])), _e(float(jP[b])), temps[ti]))
+
+
+def hist_moments(h, nbins: int, xmin: float, dx: float):
+    """Mean, variance, skewness, excess kurtosis of a density histogram
+    (analysis_pt.cpp:61-81)."""
+    h = [float(v) for v in h]
+    mu = 0.0
+    for b in range(nbins):
+        xc = xmin + (b + 0.5) * dx
+        mu += xc * h[b] * dx
+    var = skew = kurt = 0.0
+    for b in range(nbins):
+        xc = xmin + (b + 0.5) * dx
+        d = xc - mu
+        d2 = d * d
+        var += d2 * h[b] * dx
+        skew += d2 * d * h[b] * dx
+        kurt += d2 * d2 * h[b] * dx
+    if var > 0:
+        skew = _div(skew, var * math.sqrt(var))
+        kurt = _div(kurt, var * var) - 3.0
+    return mu, var, skew, kurt
+
+
+def write_moments(path: str, header: str, hists: np.ndarray, temps, nbins: int, xmin: float = -1.0,
+                  dx: float | None = None) -> None:
+    """{tag}_moments.dat: moments of the sample-mean histogram per
+    temperature with jackknife errors (analysis_pt.cpp:86-126)."""
+    hists = np.asarray(hists, np.float64)
+    S, NT = hists.shape[0], hists.shape[1]
+    dx = 2.0 / nbins if dx is None else dx
+    f = math.sqrt((S - 1.0) / S)
+    with open(path, "w") as out:
+        out.write("# %s\n" % header)
+        out.write("# Columns: T  mean  mean_err  var  var_err  skew  skew_err  kurt  kurt_err\n")
+        for ti in range(NT):
+            h = hists[:, ti, :]
+            full = hist_moments(_mean_rows(h), nbins, xmin, dx)
+            jk = [0.0, 0.0, 0.0, 0.0]
+            for j in range(S):
+                loo = hist_moments(_mean_rows(h, j), nbins, xmin, dx)
+                for m in range(4):
+                    jk[m] += (loo[m] - full[m]) * (loo[m] - full[m])
+            cols = []
+            for m in range(4):
+                cols += [full[m], f * math.sqrt(jk[m])]
+            out.write("%.8f\t" % temps[ti] + "\t".join(_e(c) for c in cols) + "\n")
+
+
+def write_glass_observables(outdir: str, tag: str, hists: np.ndarray, temps, N: int, nbins: int,
+                            xmin: float = -1.0, dx: float | None = None) -> None:
+    """{tag}_glass_observables.dat (chi = N<x^2>, g4 = (3 - <x^4>/<x^2>^2)/2,
+    A = Var_J[<x^2>]/<x^2>^2 with jackknife errors) and {tag}_sample_x2.dat
+    (analysis_pt.cpp:209-305)."""
+    hists = np.asarray(hists, np.float64)
+    S, NT = hists.shape[0], hists.shape[1]
+    dx = 2.0 / nbins if dx is None else dx
+    x2 = [[0.0] * NT for _ in range(S)]
+    x4 = [[0.0] * NT for _ in range(S)]
+    for s in range(S):
+        for ti in range(NT):
+            m2 = m4 = 0.0
+            for b in range(nbins):
+                xc = xmin + (b + 0.5) * dx
+                xc2 = xc * xc
+                v = float(hists[s, ti, b])
+                m2 += xc2 * v * dx
+                m4 += xc2 * xc2 * v * dx
+            x2[s][ti], x4[s][ti] = m2, m4
+    f = math.sqrt((S - 1.0) / S)
+    rows = []
+    for ti in range(NT):
+        x2f = x4f = 0.0
+        for s in range(S):
+            x2f += x2[s][ti]
+            x4f += x4[s][ti]
+        x2f = _div(x2f, S)
+        x4f = _div(x4f, S)
+        chi = N * x2f
+        g4 = 0.5 * (3.0 - _div(x4f, x2f * x2f)) if x2f > 0 else 0.0
+        x2v = 0.0
+        for s in range(S):
+            x2v += (x2[s][ti] - x2f) * (x2[s][ti] - x2f)
+        x2v = _div(x2v, S)
+        A = _div(x2v, x2f * x2f) if x2f > 0 else 0.0
+        jc = jg = jA = 0.0
+        for j in range(S):
+            lx2 = lx4 = 0.0
+            for s in range(S):
+                if s != j:
+                    lx2 += x2[s][ti]
+                    lx4 += x4[s][ti]
+            lx2 = _div(lx2, S - 1)
+            lx4 = _div(lx4, S - 1)
+            lchi = N * lx2
+            lg4 = 0.5 * (3.0 - _div(lx4, lx2 * lx2)) if lx2 > 0 else 0.0
+            jc += (lchi - chi) * (lchi - chi)
+            jg += (lg4 - g4) * (lg4 - g4)
+            lv = 0.0
+            for s in range(S):
+                if s != j:
+                    lv += (x2[s][ti] - lx2) * (x2[s][ti] - lx2)
+            lv = _div(lv, S - 1)
+            lA = _div(lv, lx2 * lx2) if lx2 > 0 else 0.0
+            jA += (lA - A) * (lA - A)
+        rows.append((temps[ti], chi, f * math.sqrt(jc), g4, f * math.sqrt(jg), A, f * math.sqrt(jA)))
+    with open(os.path.join(outdir, "%s_glass_observables.dat" % tag), "w") as out:
+        out.write("# Glass observables from %s overlap\n" % tag)
+        out.write("# chi = N*<x^2>,  g4 = 0.5*(3-<x^4>/<x^2>^2),  A = Var_J[<x^2>]/<x^2>^2\n")
+        out.write("# Columns: T  chi  chi_err  g4  g4_err  A  A_err\n")
+        for r in rows:
+            out.write("%.8f\t" % r[0] + "\t".join(_e(c) for c in r[1:]) + "\n")
+    with open(os.path.join(outdir, "%s_sample_x2.dat" % tag), "w") as out:
+        out.write("# Per-sample <x^2> for %s\n" % tag)
+        out.write("# Columns: T  sample_0  sample_1  ...  sample_{n-1}\n")
+        for ti in range(NT):
+            out.write("%.8f" % temps[ti] + "".join("\t" + _e(x2[s][ti]) for s in range(S)) + "\n")
+
+
+# the three distributions: file stem / tag, moments header, distribution header
+DISTRIBUTIONS = (("parisi", "Moments of P(q)", PARISI_HEADER),
+                 ("ifo", "Moments of P(C) [IFO]", IFO_HEADER),
+                 ("exp_ifo", "Moments of P(C) [exp-IFO]", EXP_IFO_HEADER))
+
+
+def write_all(outdir: str, hists: dict, temps, N: int, NT: int, nrep: int, nbins: int) -> list[str]:
+    """Every file analysis_pt writes from the overlap histograms, for the tags
+    in hists ({tag: [nsamples, NT, nbins] densities}); returns the paths."""
+    os.makedirs(outdir, exist_ok=True)
+    paths = []
+    for tag, mheader, header in DISTRIBUTIONS:
+        if tag not in hists:
+            continue
+        name = "parisi_overlap.dat" if tag == "parisi" else "%s_overlap.dat" % tag
+        write_parisi_overlap(os.path.join(outdir, name), hists[tag], temps, N, NT, nrep, nbins, header=header)
+        write_moments(os.path.join(outdir, "%s_moments.dat" % tag), mheader, hists[tag], temps, nbins)
+        write_glass_observables(outdir, tag, hists[tag], temps, N, nbins)
+        paths += [name, "%s_moments.dat" % tag, "%s_glass_observables.dat" % tag, "%s_sample_x2.dat" % tag]
+    return [os.path.join(outdir, p) for p in paths]
 
 
 def main(argv=None) -> int:
@@ -167,11 +338,9 @@ def main(argv=None) -> int:
         ifo.append(i)
         exp_ifo.append(e)
     temps = temperatures(runs[0][1], a.NT)
-    os.makedirs(a.out, exist_ok=True)
-    for name, h, header in (("parisi_overlap.dat", hists, PARISI_HEADER), ("ifo_overlap.dat", ifo, IFO_HEADER),
-                            ("exp_ifo_overlap.dat", exp_ifo, EXP_IFO_HEADER)):
-        path = os.path.join(a.out, name)
-        write_parisi_overlap(path, np.stack(h), temps, a.N, a.NT, a.nrep, a.nbins, header=header)
+    paths = write_all(a.out, {"parisi": np.stack(hists), "ifo": np.stack(ifo), "exp_ifo": np.stack(exp_ifo)},
+                      temps, a.N, a.NT, a.nrep, a.nbins)
+    for path in paths:
         print("%d samples, written %s" % (len(runs), path))
     return 0
 

@@ -1,7 +1,9 @@
 """Host parts of the GPU overlap analyses: configs.bin and energy_accept.txt
 reading, run discovery, the jackknife / file format of parisi_overlap.dat
-(analysis_pt.cpp:1418-1480), and the IFO arithmetic order checked against
-the reference analysis_pt, on synthetic files."""
+(analysis_pt.cpp:1418-1480), and every file analysis_pt derives from the
+P(q), IFO and experimental-IFO histograms (distributions, moments, glass
+observables, per-sample <x^2>) checked byte for byte against the reference
+analysis_pt, on synthetic files."""
 import math
 import os
 import subprocess
@@ -129,20 +131,43 @@ REF_ANALYSIS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__fi
                             "analysis_pt")
 
 
+def _pq_restated(cfg, nbins):
+    """P(q) densities [NT, nbins] in pspin_overlap_counts' operation order
+    (analysis_pt.cpp:1385-1424)."""
+    nsnap, NT, nrep, N, _ = cfg.shape
+    qmin, dq = -1.0, 2.0 / nbins
+    out = np.zeros((NT, nbins))
+    for t in range(NT):
+        cnt = [0] * nbins
+        for sn in range(nsnap):
+            for a in range(nrep):
+                for b in range(a + 1, nrep):
+                    s = 0.0
+                    for k in range(N):
+                        x, y = cfg[sn, t, a, k], cfg[sn, t, b, k]
+                        s = s + (x[0] * y[0] + x[1] * y[1])
+                    cnt[min(max(int((s / N - qmin) / dq), 0), nbins - 1)] += 1
+        out[t] = np.array(cnt) / (nsnap * nrep * (nrep - 1) // 2 * dq)
+    return out
+
+
 @pytest.mark.skipif(not os.path.exists(REF_ANALYSIS), reason="reference analysis_pt not built")
-def test_ifo_restatement_matches_analysis_pt(tmp_path):
-    """The operation order of pspin_ifo_counts, restated on the CPU, gives
-    ifo_overlap.dat and exp_ifo_overlap.dat identical to the reference
-    analysis_pt's on synthetic runs, including an overlap of exactly 1 (two
-    identical replicas: the last bin) and a replica with no fluctuation (zero
-    norm: skipped and not counted)."""
-    N, NT, nrep, nsnap, S, nbins = 6, 3, 3, 5, 4, 20
-    rng = np.random.default_rng(5)
+@pytest.mark.parametrize("S", [4, 1])
+def test_overlap_files_match_analysis_pt(tmp_path, S):
+    """The operation order of pspin_overlap_counts and pspin_ifo_counts,
+    restated on the CPU, and analysis.write_all (distributions, moments,
+    glass observables, per-sample <x^2>) give the same twelve files as the
+    reference analysis_pt on synthetic runs, byte for byte: including an
+    overlap of exactly 1 (two identical replicas: the last bin), a replica
+    with no fluctuation (zero norm: skipped and not counted) and, with one
+    sample, the reference's -nan jackknife errors."""
+    N, NT, nrep, nsnap, nbins = 6, 3, 3, 5, 20
+    rng = np.random.default_rng(5 + S)
     cfgs = []
     for s in range(S):
         d = tmp_path / "data" / f"PT_N{N}_a0.5_Rinf_a00.5_NT{NT}_NR{nrep}_S{s}"
         cfg = _fake_run(str(d), N, NT, nrep, nsnap, rng, s)
-        if s == 1:
+        if s == S - 1:
             cfg[:, 0, 2] = cfg[:, 0, 1]
             cfg[:, 1, 0] = cfg[0, 1, 0]
             with open(d / "configs.bin", "wb") as f:
@@ -164,11 +189,16 @@ def test_ifo_restatement_matches_analysis_pt(tmp_path):
     p = subprocess.run([REF_ANALYSIS, "-N", str(N), "-NT", str(NT), "-nrep", str(nrep), "-nbins", str(nbins)],
                        cwd=tmp_path, capture_output=True, text=True, timeout=120)
     assert p.returncode == 0, p.stderr[-1000:]
-    res = [_ifo_restated(c, nbins) for c in cfgs]
+    ifo = [_ifo_restated(c, nbins) for c in cfgs]
+    hists = {"parisi": np.stack([_pq_restated(c, nbins) for c in cfgs]),
+             "ifo": np.stack([r[0] for r in ifo]), "exp_ifo": np.stack([r[1] for r in ifo])}
     temps = A.temperatures(str(tmp_path / "data" / f"PT_N{N}_a0.5_Rinf_a00.5_NT{NT}_NR{nrep}_S0"), NT)
-    for i, (name, header) in enumerate((("ifo_overlap.dat", A.IFO_HEADER), ("exp_ifo_overlap.dat", A.EXP_IFO_HEADER))):
-        ours = tmp_path / ("ours_" + name)
-        A.write_parisi_overlap(str(ours), np.stack([r[i] for r in res]), temps, N, NT, nrep, nbins, header=header)
-        refs = [os.path.join(r, f) for r, _, fs in os.walk(tmp_path / "analysis") for f in fs if f == name]
-        assert len(refs) == 1
-        assert open(ours).read() == open(refs[0]).read(), name
+    paths = A.write_all(str(tmp_path / "ours"), hists, temps, N, NT, nrep, nbins)
+    assert len(paths) == 12
+    refdir = [r for r, _, fs in os.walk(tmp_path / "analysis") if "parisi_overlap.dat" in fs]
+    assert len(refdir) == 1
+    for path in paths:
+        ref = os.path.join(refdir[0], os.path.basename(path))
+        assert open(path).read() == open(ref).read(), os.path.basename(path)
+    if S == 1:
+        assert "-nan" in open(paths[1]).read()

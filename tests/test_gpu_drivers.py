@@ -119,8 +119,9 @@ def test_gpu_overlap_distribution_matches_analysis_pt(tmp_path):
     configurations on the GPU (pspin_overlap_counts, pspin_ifo_counts +
     cuda_pspin_b200.analysis) equal the reference analysis_pt's
     parisi_overlap.dat, ifo_overlap.dat and exp_ifo_overlap.dat on the same
-    runs: same headers, bins, densities and jackknife errors, same
-    temperatures."""
+    runs (same headers, bins, densities and jackknife errors, same
+    temperatures), and the moments, glass-observable and per-sample <x^2>
+    files derived from them are the reference's byte for byte."""
     flags = ["-N", "12", "-Tmax", "1.6", "-Tmin", "0.3", "-NT", "4", "-log_temp", "-nrep", "3", "-iter", "512",
              "-pt_freq", "1", "-save_freq", "8", "-seed", "11", "-label", "0", "-batch", "6"]
     run([os.path.join(BIN, "pspin_pt"), *flags], tmp_path)
@@ -147,6 +148,11 @@ def test_gpu_overlap_distribution_matches_analysis_pt(tmp_path):
             n_rows += 1
             filled += y[1] > 0
         assert n_rows == 4 * 100 and filled > 4, name
+    refdir = [r for r, _, fs in os.walk(tmp_path / "analysis") if "parisi_overlap.dat" in fs][0]
+    for tag in ("parisi", "ifo", "exp_ifo"):
+        for suffix in ("moments.dat", "glass_observables.dat", "sample_x2.dat"):
+            name = f"{tag}_{suffix}"
+            assert open(tmp_path / "gpu" / name).read() == open(os.path.join(refdir, name)).read(), name
 
 
 SA_FLAGS = ["-N", "12", "-nrep", "3", "-Tmax", "1.6", "-Tmin", "0.3", "-ntemp", "5", "-iter", "6", "-save_freq", "16",
