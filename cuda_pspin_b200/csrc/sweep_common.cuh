@@ -201,7 +201,7 @@ __device__ __forceinline__ void accumulate_tiles(const int2* __restrict__ R2, in
         const float4* __restrict__ C = reinterpret_cast<const float4*>(R + e + 1);
         const float2* __restrict__ A = sp + lo * kRepBlock + lane;
         const int len = hi - lo;
-#pragma unroll 4
+#pragma unroll 8
         for (int t = 0; t < len; t++) {
             const float4 c = C[t];
             const float2 a = A[t * kRepBlock];
