@@ -99,10 +99,14 @@ def measure(config: str, sweeps: int | None = None, shape=None) -> dict:
     else:
         raise ValueError(config)
     moves = sum(N * R // 2 for N, R in zip(eng.Ns, eng.Rs))
+    chains = sum(eng.Rs)
     secs, w, cl = _timed(eng, run, sweeps, warmup=8 if config != "4" else 2,
                          tune_sweeps=2 if config == "4" else 8, shape=shape)
     eng.free()
-    out = {"config": config, "sweeps": sweeps, "seconds": secs, "pair_moves_per_s": moves * sweeps / secs,
+    rate = moves * sweeps / secs
+    # latency-bound configurations: time per move along one replica's chain
+    out = {"config": config, "sweeps": sweeps, "seconds": secs, "pair_moves_per_s": rate,
+           "chains": chains, "ns_per_move_per_chain": 1e9 * chains / rate,
            "warps_per_cta": w, "ctas_per_replica_block": cl, "setup_s": setup}
     ref = os.path.join(ROOT, "profiles", "reference_sm100_timing.json")
     key = REF_KEYS.get(config)
@@ -110,6 +114,7 @@ def measure(config: str, sweeps: int | None = None, shape=None) -> dict:
         r = json.load(open(ref)).get(key)
         if r:
             out["reference_pair_moves_per_s"] = r["pair_moves_per_s"]
+            out["reference_ns_per_move_per_chain"] = 1e9 * chains / r["pair_moves_per_s"]
             out["speedup_vs_reference"] = out["pair_moves_per_s"] / r["pair_moves_per_s"]
     return out
 
