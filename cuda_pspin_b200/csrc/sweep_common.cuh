@@ -186,7 +186,10 @@ __device__ __forceinline__ void accumulate_chunk(const int2* __restrict__ R, int
 
 // Field contribution of the fully connected tiles in one staged chunk
 // (16-byte records: header, then rows of 4 couplings).  One gathered
-// a_inner feeds four partners: 8 FFMA per shared-memory gather.
+// a_inner feeds four partners: 8 FFMA per shared-memory gather.  The rows
+// are unrolled by kUnroll (more gathers in flight per warp; the summation
+// order is the same for every kUnroll).
+template <int kUnroll = 8>
 __device__ __forceinline__ void accumulate_tiles(const int2* __restrict__ R2, int n,
                                                  const float2* __restrict__ sp, int lane,
                                                  float& hx, float& hy) {
@@ -201,7 +204,7 @@ __device__ __forceinline__ void accumulate_tiles(const int2* __restrict__ R2, in
         const float4* __restrict__ C = reinterpret_cast<const float4*>(R + e + 1);
         const float2* __restrict__ A = sp + lo * kRepBlock + lane;
         const int len = hi - lo;
-#pragma unroll 8
+#pragma unroll kUnroll
         for (int t = 0; t < len; t++) {
             const float4 c = C[t];
             const float2 a = A[t * kRepBlock];
