@@ -34,6 +34,9 @@ PROPOSAL_PLAIN_FIELDS = 1
 PROPOSAL_LEARNED = 2
 MLP_PARAMS = 6426
 RECORD_FLOATS = 11
+PSPIN_OK = 0
+PSPIN_ERR_ARG = 1
+PSPIN_ERR_TIMEOUT = 8
 _STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_CURAND", 4: "ERR_ALLOC", 5: "ERR_STATE",
            6: "ERR_NUMERIC", 7: "ERR_UNSUPPORTED", 8: "ERR_TIMEOUT"}
 
@@ -61,7 +64,9 @@ class Options(ctypes.Structure):
                 ("warps_per_unit", ctypes.c_int), ("trace_sample", ctypes.c_int),
                 ("trace_replica", ctypes.c_int), ("trace_capacity", ctypes.c_int),
                 ("quiet", ctypes.c_int), ("generic_lists", ctypes.c_int), ("graph_steps", ctypes.c_int),
-                ("resync_method", ctypes.c_int), ("cluster_size", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+                ("resync_method", ctypes.c_int), ("cluster_size", ctypes.c_int),
+                ("wait_limit_clocks", ctypes.c_int), ("test_stall_move", ctypes.c_int),
+                ("reserved", ctypes.c_int * 1)]
 
 
 class Info(ctypes.Structure):
@@ -183,9 +188,11 @@ def parse_args(argv: list[str]) -> SimConfig:
 def make_options(init_exact: bool = False, resync_every: int = 0, warps_per_unit: int = 0,
                  trace: tuple[int, int, int] | None = None, quiet: bool = True,
                  generic_lists: bool = False, graph_steps: int = 0, resync_method: int = 0,
-                 cluster_size: int = 0) -> Options:
+                 cluster_size: int = 0, wait_limit_clocks: int = 0, test_stall_move: int = 0) -> Options:
     o = Options()
     o.cluster_size = int(cluster_size)
+    o.wait_limit_clocks = int(wait_limit_clocks)
+    o.test_stall_move = int(test_stall_move)
     o.resync_method = int(resync_method)
     o.generic_lists = int(generic_lists)
     o.graph_steps = int(graph_steps)

@@ -25,7 +25,32 @@ HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "noalloc.cu", "sweep_cluster.cu", "sweep_resident.cu", "analysis.cu", "tcfield.cu", "learned.cu", "layout.cpp"]
-CUTLASS = "/opt/prime-rl/.venv/lib/python3.12/site-packages/flashinfer/data/cutlass"
+
+
+def cutlass_dir() -> str:
+    """The CUTLASS 4 header tree (sm100 collectives) for tcfield.cu: the
+    CUTLASS_DIR environment variable, else the copy the flashinfer package
+    ships under its data directory (located without importing it)."""
+    d = os.environ.get("CUTLASS_DIR")
+    where = "CUTLASS_DIR"
+    if not d:
+        import importlib.util
+        spec = importlib.util.find_spec("flashinfer")
+        if spec is not None and spec.origin:
+            d = os.path.join(os.path.dirname(spec.origin), "data", "cutlass")
+            where = "the flashinfer package's data/cutlass"
+    if not d or not os.path.isfile(os.path.join(d, "include", "cutlass", "cutlass.h")):
+        raise RuntimeError(f"CUTLASS headers not found (looked at {where}: {d!r}); set CUTLASS_DIR to a "
+                           "CUTLASS 4.x checkout containing include/cutlass/cutlass.h")
+    return d
+
+
+def reference_dir() -> str:
+    """The reference checkout (giacomotrinca/cuda_pspin) that the oracle's
+    reference rebuild compiles from: PSPIN_REF, else /root/reference."""
+    return os.environ.get("PSPIN_REF", "/root/reference")
+
+
 DRIVERS = {
     "pspin_pt": ["drivers/pt_main.cpp"],
     "pspin_pt_sparse": ["drivers/pt_sparse_main.cpp"],
@@ -55,8 +80,9 @@ def build_lib(force: bool = False) -> str:
     out = os.path.join(LIB_DIR, "libpspin.so")
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(ROOT, "include", "pspin.h"))
+    cutlass = cutlass_dir()
     flags = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-ccbin", HOST_CXX,
-             f"-I{CUTLASS}/include", f"-I{CUTLASS}/tools/util/include", "--expt-relaxed-constexpr",
+             f"-I{cutlass}/include", f"-I{cutlass}/tools/util/include", "--expt-relaxed-constexpr",
              "-diag-suppress", "20012", "-Xcompiler", "-fPIC,-fopenmp,-O3"]
     if os.environ.get("PSPIN_PTXAS_V"):
         flags += ["-Xptxas", "-v"]
@@ -102,11 +128,12 @@ def build_oracle(force: bool = False) -> None:
 def build_ref() -> None:
     """Reference rebuild for sm_100a under oracle/_ref (only where the
     reference sources are present)."""
-    if not os.path.isdir("/root/reference/src"):
+    ref = reference_dir()
+    if not os.path.isdir(os.path.join(ref, "src")):
         return
     if shutil.which("make") is None:
         return
-    _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"])
+    _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", f"PSPIN_REF={ref}"])
 
 
 def main(argv: list[str] | None = None) -> int:

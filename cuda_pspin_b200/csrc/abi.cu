@@ -940,6 +940,8 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     });
     s->warps = choose_warps(s);
     if (s->warps < 0) return bail(fail(PSPIN_ERR_ARG, "warps_per_unit must be 1, 2, 4 or 8"));
+    if (s->opt.wait_limit_clocks < 0 || s->opt.test_stall_move < 0)
+        return bail(fail(PSPIN_ERR_ARG, "wait_limit_clocks and test_stall_move must be >= 0"));
     for (const SampleHost& h : s->hs) s->max_site_entries = std::max<int64_t>(s->max_site_entries, h.site_entries);
     {
         const int c = s->opt.cluster_size == 0 ? 1 : s->opt.cluster_size;
@@ -1061,6 +1063,8 @@ static int enqueue_step(pspin_state* s, int nsweeps, bool exchange, cudaEvent_t 
     p.trace_sweep0 = s->trace_sweep0;
     p.trace = s->d_trace;
     p.status = s->d_status;
+    p.wait_clocks = s->opt.wait_limit_clocks > 0 ? (long long)s->opt.wait_limit_clocks : kWaitClocks;
+    p.stall_move = s->opt.test_stall_move > 0 ? s->opt.test_stall_move - 1 : -1;
     if (e0) CK(cudaEventRecord(e0, s->st));
     p.cluster = s->proposal == PSPIN_PROPOSAL_PLAIN ? s->cluster : s->cluster2;
     if (s->proposal == PSPIN_PROPOSAL_PLAIN && s->cluster == 0) {
@@ -1185,10 +1189,18 @@ static int capture_graph(pspin_state* s, int G) {
     return PSPIN_OK;
 }
 
+static int timeout_error(int status) {
+    return fail(PSPIN_ERR_TIMEOUT,
+                "a bounded wait in the sweep kernel ran out (status %d%s): the replica blocks whose wait ran out "
+                "abandoned that launch and kept their state from before it",
+                status, (status & kStatusDrain) ? ", and the drain of its copies ran out too" : "");
+}
+
 static int run_sweeps(pspin_state* s, int nsweeps, bool pt) {
     if (!s) return fail(PSPIN_ERR_ARG, "null handle");
     if (nsweeps < 0) return fail(PSPIN_ERR_ARG, "nsweeps < 0");
     const int G = (pt && !s->profiling) ? graph_steps(s) : 0;
+    CK(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->st));   // a time-out is reported by the call it happens in
     int left = nsweeps;
     while (left > 0) {
         // whole graphs of G steps up to the next resync, from a step boundary
@@ -1224,7 +1236,7 @@ static int run_sweeps(pspin_state* s, int nsweeps, bool pt) {
     CK(cudaStreamSynchronize(s->st));
     int status = 0;
     CK(cudaMemcpy(&status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-    if (status) return fail(PSPIN_ERR_TIMEOUT, "a bounded wait in the sweep kernel expired (status %d)", status);
+    if (status) return timeout_error(status);
     return PSPIN_OK;
 }
 
@@ -1297,7 +1309,8 @@ extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int
     const float prob0 = s->rec_prob;
     s->rec_prob = 0.f;                       // trials record no training moves
     cudaEvent_t t0 = nullptr, t1 = nullptr;
-    cudaError_t e = copy_all(true);
+    cudaError_t e = cudaMemsetAsync(s->d_status, 0, sizeof(int), s->st);
+    if (e == cudaSuccess) e = copy_all(true);
     if (e == cudaSuccess) e = cudaEventCreate(&t0);
     if (e == cudaSuccess) e = cudaEventCreate(&t1);
     int best_w = w0, best_c = c0;
@@ -1337,7 +1350,7 @@ extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int
     drop_graph(s);
     if (rc != PSPIN_OK) return rc;
     if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
-    if (status) return fail(PSPIN_ERR_TIMEOUT, "a bounded wait in the sweep kernel expired (status %d)", status);
+    if (status) return timeout_error(status);
     if (chosen_warps) *chosen_warps = W;
     if (chosen_cluster) *chosen_cluster = Cl;
     return PSPIN_OK;
@@ -2171,6 +2184,8 @@ extern "C" int pspin_checkpoint_save(pspin_state* s, const char* path) {
     return PSPIN_OK;
 }
 
+// Reads and checks the whole file into host buffers before it changes
+// anything, so a rejected or truncated file leaves the handle as it was.
 extern "C" int pspin_checkpoint_load(pspin_state* s, const char* path) {
     if (!s || !path) return fail(PSPIN_ERR_ARG, "null argument");
     CkFile f;
@@ -2196,44 +2211,86 @@ extern "C" int pspin_checkpoint_load(pspin_state* s, const char* path) {
     f.get(sweeps_done); f.get(since_resync); f.get(counter); f.get(proposal);
     f.get(warps); f.get(cluster); f.get(warps2); f.get(cluster2);
     if (!f.ok || warps < 1 || warps > 8 || warps2 < 1 || warps2 > 8 || cluster < 0 || cluster > 16 || cluster2 < 1 ||
-        cluster2 > 16)
+        cluster2 > 16 || proposal < PSPIN_PROPOSAL_PLAIN || proposal > PSPIN_PROPOSAL_LEARNED)
         return fail(PSPIN_ERR_ARG, "checkpoint file is truncated or corrupt");
-    if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
-    TRY(file_to_dev(s, f, s->d_spins, (size_t)s->spin_total));
-    TRY(file_to_dev(s, f, s->d_E, (size_t)s->R_tot));
-    std::vector<double> betas(s->R_tot);
-    f.get(betas.data(), betas.size() * sizeof(double));
-    TRY(file_to_dev(s, f, s->d_target, (size_t)s->R_tot));
-    TRY(file_to_dev(s, f, s->d_acc, (size_t)s->R_tot));
-    TRY(file_to_dev(s, f, s->d_prop, (size_t)s->R_tot));
+    const size_t R = (size_t)s->R_tot;
+    std::vector<float2> spins((size_t)s->spin_total);
+    std::vector<double> E(R), betas(R), target(R);
+    std::vector<long long> acc(R), prop(R);
+    f.get(spins.data(), spins.size() * sizeof(float2));
+    f.get(E.data(), R * sizeof(double));
+    f.get(betas.data(), R * sizeof(double));
+    f.get(target.data(), R * sizeof(double));
+    f.get(acc.data(), R * sizeof(long long));
+    f.get(prop.data(), R * sizeof(long long));
     int32_t NT = 0, nrep = 0, freq = 0;
     f.get(NT); f.get(nrep); f.get(freq);
     if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
-    if (NT >= 2) {
-        std::vector<double> sched(NT);
-        f.get(sched.data(), sched.size() * sizeof(double));
-        if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
-        TRY(pspin_pt_init(s, NT, nrep, sched.data(), freq));
-        const size_t SS = s->S;
-        TRY(file_to_dev(s, f, s->d_perm, SS * NT * nrep));
-        TRY(file_to_dev(s, f, s->d_drand, SS));
-        TRY(file_to_dev(s, f, s->d_ex_acc, SS * (NT - 1)));
-        TRY(file_to_dev(s, f, s->d_ex_prop, SS * (NT - 1)));
-    }
-    CK(cudaMemcpyAsync(s->d_beta, betas.data(), betas.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
-    int32_t has_net = 0;
+    if (NT == 1 || NT < 0 || (NT >= 2 && (nrep < 1 || freq < 1)))
+        return fail(PSPIN_ERR_ARG, "checkpoint file is corrupt (PT shape NT=%d nrep=%d pt_freq=%d)", NT, nrep, freq);
+    if (NT >= 2)
+        for (const SampleHost& h : s->hs)
+            if (h.R != NT * nrep) return fail(PSPIN_ERR_ARG, "checkpoint PT shape does not match the samples' replicas");
+    const size_t SS = s->S, nt = NT >= 2 ? (size_t)NT : 0, nr = NT >= 2 ? (size_t)nrep : 0;
+    std::vector<double> sched(nt);
+    std::vector<int> perm(SS * nt * nr);
+    std::vector<unsigned long long> drand(nt ? SS : 0);
+    std::vector<long long> ex_acc(nt ? SS * (nt - 1) : 0), ex_prop(ex_acc.size());
+    f.get(sched.data(), sched.size() * sizeof(double));
+    f.get(perm.data(), perm.size() * sizeof(int));
+    f.get(drand.data(), drand.size() * sizeof(unsigned long long));
+    f.get(ex_acc.data(), ex_acc.size() * sizeof(long long));
+    f.get(ex_prop.data(), ex_prop.size() * sizeof(long long));
+    int32_t has_net = 0, adam_t = 0, cap = 0;
+    uint64_t lseed = 0;
+    float prob = 0.f;
     f.get(has_net);
+    std::vector<float> w32, am, av;
+    if (f.ok && has_net) {
+        f.get(adam_t); f.get(lseed); f.get(prob); f.get(cap);
+        w32.resize(kMlpParamsHost);
+        am.resize(kMlpParamsHost);
+        av.resize(kMlpParamsHost);
+        f.get(w32.data(), w32.size() * sizeof(float));
+        f.get(am.data(), am.size() * sizeof(float));
+        f.get(av.data(), av.size() * sizeof(float));
+    }
     if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
+    if (fgetc(f.f) != EOF) return fail(PSPIN_ERR_ARG, "checkpoint file has trailing bytes (corrupt)");
+    for (size_t i = 0; i < perm.size(); i++)
+        if (perm[i] < 0 || perm[i] >= NT * nrep) return fail(PSPIN_ERR_ARG, "checkpoint file is corrupt (perm)");
+    if (proposal == PSPIN_PROPOSAL_LEARNED && !has_net && !s->d_w32)
+        return fail(PSPIN_ERR_ARG, "checkpoint uses the learned proposal but holds no network");
+
+    // ---- everything checked: apply
+    drop_graph(s);
+    CK(cudaMemcpyAsync(s->d_spins, spins.data(), spins.size() * sizeof(float2), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->d_E, E.data(), R * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->d_target, target.data(), R * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->d_acc, acc.data(), R * sizeof(long long), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->d_prop, prop.data(), R * sizeof(long long), cudaMemcpyHostToDevice, s->st));
+    if (NT >= 2) {
+        TRY(pspin_pt_init(s, NT, nrep, sched.data(), freq));
+        CK(cudaMemcpyAsync(s->d_perm, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice, s->st));
+        CK(cudaMemcpyAsync(s->d_drand, drand.data(), drand.size() * sizeof(unsigned long long),
+                           cudaMemcpyHostToDevice, s->st));
+        CK(cudaMemcpyAsync(s->d_ex_acc, ex_acc.data(), ex_acc.size() * sizeof(long long), cudaMemcpyHostToDevice, s->st));
+        CK(cudaMemcpyAsync(s->d_ex_prop, ex_prop.data(), ex_prop.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                           s->st));
+    } else if (s->pt_NT >= 2) {
+        // the saved chain ran without PT: the handle's PT state would resume with a wrong perm
+        CK(cudaStreamSynchronize(s->st));
+        cudaFree(s->d_beta_sched); cudaFree(s->d_perm); cudaFree(s->d_drand); cudaFree(s->d_ex_acc); cudaFree(s->d_ex_prop);
+        s->d_beta_sched = nullptr; s->d_perm = nullptr; s->d_drand = nullptr; s->d_ex_acc = nullptr; s->d_ex_prop = nullptr;
+        s->pt_NT = s->pt_nrep = s->pt_freq = 0;
+        s->obs_cap = 0;
+    }
+    CK(cudaMemcpyAsync(s->d_beta, betas.data(), R * sizeof(double), cudaMemcpyHostToDevice, s->st));
     if (has_net) {
-        int32_t adam_t = 0, cap = 0;
-        uint64_t seed = 0;
-        float prob = 0.f;
-        f.get(adam_t); f.get(seed); f.get(prob); f.get(cap);
-        if (!f.ok) return fail(PSPIN_ERR_ARG, "checkpoint file is truncated");
-        TRY(pspin_learn_init(s, seed, std::max(cap, 1), prob));
-        TRY(file_to_dev(s, f, s->d_w32, (size_t)kMlpParamsHost));
-        TRY(file_to_dev(s, f, s->d_adam_m, (size_t)kMlpParamsHost));
-        TRY(file_to_dev(s, f, s->d_adam_v, (size_t)kMlpParamsHost));
+        TRY(pspin_learn_init(s, lseed, std::max(cap, 1), prob));
+        CK(cudaMemcpyAsync(s->d_w32, w32.data(), w32.size() * sizeof(float), cudaMemcpyHostToDevice, s->st));
+        CK(cudaMemcpyAsync(s->d_adam_m, am.data(), am.size() * sizeof(float), cudaMemcpyHostToDevice, s->st));
+        CK(cudaMemcpyAsync(s->d_adam_v, av.data(), av.size() * sizeof(float), cudaMemcpyHostToDevice, s->st));
         CK(launch_to_bf16(s->d_w32, s->d_wbf, s->st));
         s->adam_t = adam_t;
     }

@@ -52,6 +52,15 @@ constexpr int kStage = 256;       // max entries per TMA chunk (2 KB)
 constexpr int kStages = 3;        // chunks in flight per warp
 constexpr int kRepBlock = 32;     // replicas per unit (one per lane)
 
+// Status word bits raised by the sweep kernels.  A CTA (or cluster) whose
+// bounded wait ran out stops issuing copies, drains the copies in flight,
+// and leaves its replicas' amplitudes, energies and counters as they were
+// before the launch.
+constexpr int kStatusTimeout = 1;          // a ring wait ran out; the block aborted the launch
+constexpr int kStatusDrain = 2;            // the drain of in-flight copies ran out as well
+constexpr long long kWaitClocks = 1ll << 31;   // default ring-wait limit (~1 s at 1.9 GHz)
+constexpr long long kDrainClocks = 1ll << 31;  // drain limit after an abort
+
 struct SampleDev {
     int N;
     int R;                 // replicas of this sample
@@ -102,7 +111,9 @@ struct SweepParams {
     int trace_sample, trace_rep, trace_cap;
     long long trace_sweep0;
     void* trace;                      // pspin_move_record*
-    int* status;                      // error word (bounded waits, bad sizes)
+    int* status;                      // error word (kStatus* bits)
+    long long wait_clocks;            // ring-wait limit in SM clocks
+    int stall_move;                   // tests: move index of the stall wait (-1: none)
 };
 
 // shared memory bytes of one sweep CTA: amplitudes, per-warp field

@@ -158,8 +158,9 @@ __host__ __device__ inline size_t learned_cluster_buffer_offset(int N, int warps
     return (learned_base_bytes(N, warps) + 15) & ~(size_t)15;
 }
 
+// cluster variant: the exchange buffer, then the cluster's abort flag (one word)
 inline size_t learned_smem_bytes(int N, int warps, int C = 1) {
-    if (C > 1) return learned_cluster_buffer_offset(N, warps) + (size_t)2 * C * kRepBlock * sizeof(float4);
+    if (C > 1) return learned_cluster_buffer_offset(N, warps) + (size_t)2 * C * kRepBlock * sizeof(float4) + 16;
     return learned_base_bytes(N, warps);
 }
 
@@ -192,6 +193,7 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
     float* xch = reinterpret_cast<float*>(bufB + kMlpBufWords);
     auto out_of = [&](int o) { return outs[o * kOutStride + lane]; };
     float4* cred = CL ? reinterpret_cast<float4*>(smem_raw + learned_cluster_buffer_offset(N, W)) : nullptr;
+    int* cflag = CL ? reinterpret_cast<int*>(cred + (size_t)2 * C * kRepBlock) : nullptr;   // cluster abort flag
 
     const bool active = lane < U.rep_count;
     const int64_t gr = S.rep_off + U.rep_begin + lane;
@@ -202,6 +204,7 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
         sp[idx] = v;
     }
     if (threadIdx.x < kRepBlock) sp[N * kRepBlock + threadIdx.x] = make_float2(1.f, 0.f);
+    if (CL && threadIdx.x == 0) *cflag = 0;
 
     double E = 0.0, beta_d = 0.0;
     float beta = 0.f;
@@ -253,19 +256,26 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
         st.next(pc);
     };
     for (int s = 0; s < kLStages; s++) issue();
+    __shared__ __align__(8) uint64_t stall_bar;      // test hook: nothing arrives on it
+    if (threadIdx.x == 0 && P.stall_move >= 0) {
+        mbar_init(&stall_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
     if (CL) cluster_sync();                    // every CTA runs before the first remote store
     uint32_t xchg = 0;                         // exchanges so far (buffer parity)
+    bool aborted = false;                      // set uniformly over the CTA (cluster) by reduce()
 
     // one pass over this warp's share of two lists: the sites' lists (base 0)
     // or the pair's sub-lists (base 2, always in the group format)
     auto pass = [&](int m, int base, float* h) {
-        for (int which = base; which < base + 2; which++) {
+        for (int which = base; which < base + 2 && ok_wait; which++) {
             int c, c_end;
             st.range(m, which, c, c_end);
             for (; c < c_end; c++) {
                 const uint32_t slot = consumed % kLStages;
-                if (ok_wait) ok_wait = mbar_wait(bars + slot, (consumed / kLStages) & 1u, P.status);
+                ok_wait = ring_wait(bars + slot, (consumed / kLStages) & 1u, P.status, P.wait_clocks);
+                if (!ok_wait) break;               // stop consuming and issuing; abort in reduce()
                 const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
                 const int k2 = 2 * (which & 1);
                 if (S.fc_tiles && which < 2)       // unrolled by 2: the kernel is held to 80 registers
@@ -278,11 +288,17 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
             }
         }
     };
-    // partial sums of all warps (and all CTAs of the cluster) -> warp 0
+    // partial sums of all warps (and all CTAs of the cluster) -> warp 0.
+    // Also agrees on an abort: a warp whose wait ran out makes the whole CTA
+    // (and, through the flag, the whole cluster) set `aborted` here.
     auto reduce = [&](const float* h) {
         red[warp * kRepBlock + lane] = make_float4(h[0], h[1], h[2], h[3]);
-        __syncthreads();
+        const bool bad = __syncthreads_or(!ok_wait);
         float4 hs = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!CL && bad) {
+            aborted = true;
+            return hs;
+        }
         if (warp == 0)
             for (int w = 0; w < W; w++) {
                 const float4 v = red[w * kRepBlock + lane];
@@ -290,9 +306,16 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
             }
         if (CL) {
             float4* buf = cred + (size_t)(xchg & 1u) * C * kRepBlock;
-            if (warp == 0)
+            if (warp == 0) {
                 for (int q = 0; q < C; q++) st_cluster_f4(buf + rank * kRepBlock + lane, (uint32_t)q, hs);
+                if (bad && lane == 0)
+                    for (int q = 0; q < C; q++) st_cluster_u32(cflag, (uint32_t)q, 1u);
+            }
             cluster_sync();
+            if (*(volatile int*)cflag) {
+                aborted = true;
+                return hs;
+            }
             if (warp == 0) {
                 hs = buf[lane];
                 for (int q = 1; q < C; q++) {
@@ -313,8 +336,10 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
 
         // ---- fields at x: h_i (with a_j), h_j (with a_i) ---------------------------
         float h[4] = {0.f, 0.f, 0.f, 0.f};
+        if (m == P.stall_move) ok_wait = stall_wait(&stall_bar, P.status, P.wait_clocks);
         pass(m, 0, h);
         const float4 hs1 = reduce(h);
+        if (aborted) break;
         float2 ai = make_float2(0.f, 0.f), aj = ai, ain = ai, ajn = ai;
         const float2 hi1 = make_float2(hs1.x, hs1.y), hj1 = make_float2(hs1.z, hs1.w);
         float cu = 0.f, lq_fwd = 0.f, lq_ratio = 0.f, tn = 0.5f, psi_i = 0.f, psi_j = 0.f, Ssum = 1.f;
@@ -386,6 +411,7 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
         h[0] = h[1] = h[2] = h[3] = 0.f;
         pass(m, 2, h);
         const float4 dh = reduce(h);
+        if (aborted) break;
         float dE = 0.f;
         float2 hi2 = hi1, hj2 = hj1;
         if (warp == 0) {
@@ -465,9 +491,8 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
         }
         __syncthreads();
     }
-    if (!ok_wait && lane == 0)
-        for (uint32_t q = consumed; q < issued; q++) mbar_wait(bars + q % kLStages, (q / kLStages) & 1u, P.status);
-    if (writer) {
+    if (aborted) drain_ring(bars, kLStages, consumed, issued, P.status);   // state stays as before the launch
+    if (writer && !aborted) {
         for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
             const int site = idx >> 5, l = idx & 31;
             if (l < U.rep_count) P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l] = sp[idx];

@@ -1,9 +1,10 @@
 // noalloc.cu -- FMC survivor counting that allocates nothing.
 //
-// Some callers cannot call cudaMalloc: code running while a stream is being
-// captured into a CUDA graph, host frameworks that own every device
-// allocation through their own pool, or plugins that only receive device
-// pointers from their host.  pspin_fmc_survivors_static counts the
+// Some callers cannot call cudaMalloc: host frameworks that own every
+// device allocation through their own pool (a second allocator would
+// fragment or overcommit the memory the pool has reserved), and plugins
+// that only receive device pointers from their host and may not take
+// device memory of their own.  pspin_fmc_survivors_static counts the
 // quartet-channel pairs that survive the frequency-matching filter (the
 // count the sparse set-up draws its quartets from) with its intermediate
 // per-row counts in a file-scope device array instead of a cudaMalloc'd
@@ -20,7 +21,9 @@
 //    different host threads on one device) race on it.
 //  * The device address of the array is looked up with
 //    cudaGetSymbolAddress by the first call on each device (with that
-//    device current); make that first call before any stream capture.
+//    device current) and kept for that device's CUDA context; a call in a
+//    new context (after cudaDeviceReset, say) looks it up again.  Make the
+//    first call on a device before any stream capture.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -105,6 +108,35 @@ __global__ void survivor_sum_kernel(const unsigned long long* rows, int N, int64
 
 static std::mutex g_addr_mu;
 static unsigned long long* g_addr[kMaxDevices] = {};
+static unsigned long long g_ctx_id[kMaxDevices] = {};   // context the cached address belongs to
+
+// Unique id of the calling thread's current CUDA context (ids are never
+// reused within a process), through driver entry points the runtime hands
+// out; 0 when there is no current context or the entry points are missing.
+static unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        looked_up = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess)
+            get_current = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q2) != cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess)
+            get_id = nullptr;
+        cudaGetLastError();
+    }
+    if (!get_current || !get_id) return 0;
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != 0 || !ctx) return 0;
+    if (get_id(ctx, &id) != 0) return 0;
+    return id;
+}
 
 }  // namespace pspin
 
@@ -133,15 +165,18 @@ extern "C" int pspin_fmc_survivors_static(int N, const double* d_omega, double g
     unsigned long long* rows = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_addr_mu);
-        if (!g_addr[dev]) {
+        const unsigned long long ctx = current_context_id();
+        if (!g_addr[dev] || ctx == 0 || ctx != g_ctx_id[dev]) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_survivor_rows);
             if (e != cudaSuccess || !p) {
+                g_addr[dev] = nullptr;
                 return report_error(PSPIN_ERR_CUDA,
                                     std::string("pspin_fmc_survivors_static: cudaGetSymbolAddress failed: ") +
                                         cudaGetErrorString(e));
             }
             g_addr[dev] = static_cast<unsigned long long*>(p);
+            g_ctx_id[dev] = current_context_id();   // the look-up made the context current if it was not
         }
         rows = g_addr[dev];
     }

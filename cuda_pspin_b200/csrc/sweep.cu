@@ -126,20 +126,28 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepParams P) {
         sp[cj0 * kRepBlock + lane] = cajn;     // h_i is evaluated at the proposed a_j
     };
 
+    __shared__ __align__(8) uint64_t stall_bar;      // test hook: nothing arrives on it
+    if (threadIdx.x == 0 && P.stall_move >= 0) {
+        mbar_init(&stall_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
     if (warp == 0 && total > 0) prepare(0);
     __syncthreads();
 
+    bool aborted = false;
     for (int m = 0; m < total; m++) {
         const long long sw = sweep0 + m / steps;
         const int k = m % steps;
         float h[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int which = 0; which < 2; which++) {
+        if (m == P.stall_move) ok = stall_wait(&stall_bar, P.status, P.wait_clocks);
+        for (int which = 0; which < 2 && ok; which++) {
             int c, c_end;
             st.range(m, which, c, c_end);
             for (; c < c_end; c++) {
                 const uint32_t slot = consumed % kStages;
-                if (ok) ok = mbar_wait(bars + slot, (consumed / kStages) & 1u, P.status);
+                ok = ring_wait(bars + slot, (consumed / kStages) & 1u, P.status, P.wait_clocks);
+                if (!ok) break;                    // stop consuming and issuing; abort below
                 const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
                 if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
                 else accumulate_chunk(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
@@ -150,7 +158,10 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepParams P) {
             }
         }
         red[warp * kRepBlock + lane] = make_float4(h[0], h[1], h[2], h[3]);
-        __syncthreads();
+        if (__syncthreads_or(!ok)) {              // CTA-uniform: every warp leaves at this move
+            aborted = true;
+            break;
+        }
 
         if (warp == 0) {
             float4 hs = red[lane];
@@ -194,9 +205,12 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepParams P) {
         }
         __syncthreads();
     }
-    // copies still in flight after a time-out: wait for them (bounded)
-    if (!ok && lane == 0)
-        for (uint32_t k = consumed; k < issued; k++) mbar_wait(bars + k % kStages, (k / kStages) & 1u, P.status);
+    if (aborted) {
+        // copies still in flight: wait for them (bounded); the replicas keep
+        // their state from before the launch
+        drain_ring(bars, kStages, consumed, issued, P.status);
+        return;
+    }
 
     for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
         const int site = idx >> 5, l = idx & 31;

@@ -28,8 +28,9 @@ __host__ __device__ inline size_t cluster_buffer_offset(int N, int warps) {
     return (sweep_smem_bytes(N, warps) + 15) & ~(size_t)15;
 }
 
+// exchange buffer [2][C][32] float4, then the cluster's abort flag (one word)
 inline size_t cluster_smem_bytes(int N, int warps, int C) {
-    return cluster_buffer_offset(N, warps) + (size_t)2 * C * kRepBlock * sizeof(float4);
+    return cluster_buffer_offset(N, warps) + (size_t)2 * C * kRepBlock * sizeof(float4) + 16;
 }
 
 template <int VARIANT>
@@ -51,6 +52,8 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     uint64_t* bars_all = reinterpret_cast<uint64_t*>(ring_all + (size_t)W * kStages * kStage);
     uint64_t* bars = bars_all + warp * kStages;
     float4* cred = reinterpret_cast<float4*>(smem_raw + cluster_buffer_offset(N, W));   // [2][C][32]
+    // raised in every CTA of the cluster by a CTA that aborts (see below)
+    int* cflag = reinterpret_cast<int*>(cred + (size_t)2 * C * kRepBlock);
 
     const bool active = lane < U.rep_count;
     const bool writer = rank == 0;
@@ -63,6 +66,7 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
         sp[idx] = v;
     }
     if (threadIdx.x < kRepBlock) sp[N * kRepBlock + threadIdx.x] = make_float2(1.f, 0.f);  // virtual site
+    if (threadIdx.x == 0) *cflag = 0;
 
     double E = 0.0, beta_d = 0.0;
     float beta = 0.f;
@@ -131,21 +135,29 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
         sp[cj0 * kRepBlock + lane] = cajn;     // h_i is evaluated at the proposed a_j
     };
 
+    __shared__ __align__(8) uint64_t stall_bar;      // test hook: nothing arrives on it
+    if (threadIdx.x == 0 && P.stall_move >= 0) {
+        mbar_init(&stall_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
     if (warp == 0 && total > 0) prepare(0);
     __syncthreads();
     cluster_sync();                            // every CTA runs before the first remote store
 
+    bool aborted = false;
     for (int m = 0; m < total; m++) {
         const long long sw = sweep0 + m / steps;
         const int k = m % steps;
         float h[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int which = 0; which < 2; which++) {
+        if (m == P.stall_move) ok = stall_wait(&stall_bar, P.status, P.wait_clocks);
+        for (int which = 0; which < 2 && ok; which++) {
             int c, c_end;
             st.range(m, which, c, c_end);
             for (; c < c_end; c++) {
                 const uint32_t slot = consumed % kStages;
-                if (ok) ok = mbar_wait(bars + slot, (consumed / kStages) & 1u, P.status);
+                ok = ring_wait(bars + slot, (consumed / kStages) & 1u, P.status, P.wait_clocks);
+                if (!ok) break;                    // stop consuming and issuing; abort below
                 const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
                 if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
                 else accumulate_chunk(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
@@ -156,7 +168,7 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
             }
         }
         red[warp * kRepBlock + lane] = make_float4(h[0], h[1], h[2], h[3]);
-        __syncthreads();
+        const bool bad = __syncthreads_or(!ok);
         float4* buf = cred + (size_t)(m & 1) * C * kRepBlock;
         if (warp == 0) {
             float4 hs = red[lane];
@@ -165,8 +177,16 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
                 hs.x += v.x; hs.y += v.y; hs.z += v.z; hs.w += v.w;
             }
             for (int q = 0; q < C; q++) st_cluster_f4(buf + rank * kRepBlock + lane, (uint32_t)q, hs);
+            // an aborting CTA raises the flag in every CTA before the barrier,
+            // so all of them read it after the same barrier and leave together
+            if (bad && lane == 0)
+                for (int q = 0; q < C; q++) st_cluster_u32(cflag, (uint32_t)q, 1u);
         }
         cluster_sync();
+        if (*(volatile int*)cflag) {
+            aborted = true;
+            break;
+        }
 
         if (warp == 0) {
             float4 hs = buf[lane];
@@ -208,9 +228,8 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
         }
         __syncthreads();
     }
-    if (!ok && lane == 0)
-        for (uint32_t q = consumed; q < issued; q++) mbar_wait(bars + q % kStages, (q / kStages) & 1u, P.status);
-    if (writer) {
+    if (aborted) drain_ring(bars, kStages, consumed, issued, P.status);   // state stays as before the launch
+    if (writer && !aborted) {
         for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
             const int site = idx >> 5, l = idx & 31;
             if (l < U.rep_count) P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l] = sp[idx];

@@ -46,7 +46,9 @@ __device__ __forceinline__ void propose(float2 ai, float2 aj, U4 w, float2& ain,
 // bulk copies (cp.async.bulk, completion counted on one mbarrier per slot)
 // kStages-1 chunks ahead of the chunk being read; the pair schedule is known
 // in advance, so the prefetch runs across move boundaries.  Waits are
-// bounded: after ~2^31 clocks the kernel sets *status and stops waiting.
+// bounded (SweepParams::wait_clocks): a wait that runs out raises the status
+// word, and the CTA (every CTA of a cluster) aborts the launch at the next
+// move barrier without writing anything back.
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -78,17 +80,44 @@ __device__ __forceinline__ void fence_async_shared() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// bounded wait; returns false (and raises the status word) on time-out
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status) {
+// Bounded wait; returns false and raises `flag` in the status word when
+// `limit` SM clocks pass before the phase completes.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status, long long limit,
+                                          int flag = kStatusTimeout) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > (1ll << 31)) {
-            atomicOr(status, 1);
+        if (clock64() - t0 > limit) {
+            atomicOr(status, flag);
             return false;
         }
     }
     return true;
+}
+
+// A ring wait made warp-uniform: the warp goes on only if every lane saw
+// the copy land.
+__device__ __forceinline__ bool ring_wait(uint64_t* bar, uint32_t parity, int* status, long long limit) {
+    return __all_sync(0xffffffffu, mbar_wait(bar, parity, status, limit));
+}
+
+// After an abort: lane 0 waits (bounded) for the copies this warp issued and
+// never consumed, so that no bulk copy is still writing into shared memory
+// when the CTA exits.  Completed phases pass at once (their parity is the
+// previous phase's), so a copy whose wait gave up is waited for again here.
+__device__ __forceinline__ void drain_ring(uint64_t* bars, int stages, uint32_t consumed, uint32_t issued,
+                                           int* status) {
+    if ((threadIdx.x & 31) == 0)
+        for (uint32_t q = consumed; q < issued; q++)
+            if (!mbar_wait(bars + q % stages, (q / stages) & 1u, status, kDrainClocks, kStatusDrain)) break;
+    __syncwarp();
+}
+
+// Test hook: the bounded wait of every warp at move P.stall_move on an
+// mbarrier that nothing arrives on, so the wait runs out and the kernel
+// takes its abort path.
+__device__ __forceinline__ bool stall_wait(uint64_t* bar, int* status, long long limit) {
+    return ring_wait(bar, 0u, status, limit);
 }
 
 // Position in a warp's chunk stream: move m, list (0: site i0, 1: site j0),
@@ -249,6 +278,13 @@ __device__ __forceinline__ void st_cluster_f4(const void* local, uint32_t rank, 
     asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(ra), "f"(v.x), "f"(v.y), "f"(v.z),
                  "f"(v.w)
                  : "memory");
+}
+
+__device__ __forceinline__ void st_cluster_u32(const void* local, uint32_t rank, uint32_t v) {
+    const uint32_t la = (uint32_t)__cvta_generic_to_shared(local);
+    uint32_t ra;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(la), "r"(rank));
+    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(ra), "r"(v) : "memory");
 }
 
 }  // namespace pspin

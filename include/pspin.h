@@ -39,7 +39,9 @@ enum {
     PSPIN_ERR_STATE = 5,     /* call not valid in the handle's current state */
     PSPIN_ERR_NUMERIC = 6,   /* running energy left the FP64 resync tolerance */
     PSPIN_ERR_UNSUPPORTED = 7,
-    PSPIN_ERR_TIMEOUT = 8    /* a bounded device wait expired; results invalid */
+    PSPIN_ERR_TIMEOUT = 8    /* a bounded device wait expired: the replica blocks
+                                whose wait ran out abandoned that launch and kept
+                                their state from before it */
 };
 
 enum { PSPIN_DENSE = 0,      /* spherical constraint, dense 3-channel H4 (mc.cu)   */
@@ -95,7 +97,17 @@ typedef struct pspin_options {
                             lists resident in shared memory (small lists;
                             plain move only).  Both the plain and the
                             two-pass sweep start with this shape. */
-    int reserved[3];
+    int wait_limit_clocks; /* the sweep kernels' bounded waits on their copy
+                            rings give up after this many SM clocks; 0 ->
+                            2^31 (about one second).  A replica block whose
+                            wait runs out abandons that launch and keeps its
+                            state from before it; the call returns
+                            PSPIN_ERR_TIMEOUT. */
+    int test_stall_move; /* tests of the time-out path: k > 0 makes every CTA
+                            of the ring-fed sweep kernels wait, at move k-1
+                            of each launch, on a barrier that nothing
+                            completes, so the bounded wait runs out; 0: off */
+    int reserved[1];
 } pspin_options;
 
 typedef struct pspin_info {
@@ -281,16 +293,17 @@ int  pspin_fmc_mask(int N, const double* omega, double gamma, uint8_t* mask_out,
 int  pspin_quartet_roundtrip(int N, int64_t* n_fail);
 
 /* ---- allocation-free survivor count (no counterpart in the reference) ---
- * For callers that cannot call cudaMalloc (work recorded while a stream is
- * captured, hosts whose own pool owns all device memory, plugins handed
- * only device pointers): counts the quartet-channel pairs that pass the FMC
- * filter, like pspin_fmc_mask's n_active, without allocating.  omega[N] and
+ * For callers that cannot call cudaMalloc (hosts whose own memory pool owns
+ * all device memory, plugins handed only device pointers): counts the
+ * quartet-channel pairs that pass the FMC filter, like pspin_fmc_mask's
+ * n_active, without allocating.  omega[N] and
  * counts[4] (total, channel 0, 1, 2) are device pointers; stream is a
  * cudaStream_t (NULL: the default stream); the call is asynchronous on it.
  * Intermediate per-row counts live in one static device array sized for
  * N <= 1024 (larger N returns PSPIN_ERR_ARG).  The first call on a device
- * looks up that array's address and should come before any stream capture.
- * Calls that overlap on the GPU share the array and race. */
+ * (and the first after that device's context was reset) looks up that
+ * array's address, and should come before any stream capture.  Calls that
+ * overlap on the GPU share the array and race. */
 int  pspin_fmc_survivors_static(int N, const double* omega, double gamma, int64_t* counts,
                                 void* stream);
 

@@ -203,13 +203,61 @@ class SparseInit:
                                           self.info.h2_active, P(so), P(sn), i0, j0)
 
 
-def check_trace(ref, spins0: np.ndarray, trace: np.ndarray, tol: float = 1e-5):
+class SparseFromList:
+    """The sparse chain's energy (mc_sparse.cu:258-315) over a given quartet
+    list: for replaying traces at sizes whose oracle set-up (2*C(N,4) host
+    normals) is too large, with the list and couplings taken from a run that
+    is itself checked bit for bit against the reference's selection."""
+
+    def __init__(self, N: int, q: np.ndarray, qg: np.ndarray, g2_real: np.ndarray | None = None,
+                 h2_active: int = 0):
+        self.N = N
+        self.q = np.ascontiguousarray(q, np.int32).reshape(-1, 5)
+        self.qg = np.ascontiguousarray(qg, np.float64)
+        g2 = np.zeros((N, N, 2))
+        if g2_real is not None:
+            g2[..., 0] = g2_real
+        self.g2 = np.ascontiguousarray(g2.ravel())
+        self.h2 = int(h2_active)
+
+    def energy(self, spins_c: np.ndarray):
+        s = np.ascontiguousarray(np.stack([spins_c.real, spins_c.imag], -1).ravel())
+        q = np.ascontiguousarray(self.q.ravel())
+        e2, e4 = ctypes.c_double(), ctypes.c_double()
+        lib().orc_energy_sparse(self.N, P(self.g2), len(self.qg), P(q), P(self.qg), self.h2, P(s),
+                                ctypes.byref(e2), ctypes.byref(e4))
+        return e2.value, e4.value
+
+    def abs_terms(self, old_c, new_c, i0, j0) -> float:
+        so = np.ascontiguousarray(np.stack([old_c.real, old_c.imag], -1).ravel())
+        sn = np.ascontiguousarray(np.stack([new_c.real, new_c.imag], -1).ravel())
+        q = np.ascontiguousarray(self.q.ravel())
+        return lib().orc_sparse_abs_terms(self.N, P(self.g2), len(self.qg), P(q), P(self.qg), self.h2,
+                                          P(so), P(sn), i0, j0)
+
+
+def check_trace(ref, spins0: np.ndarray, trace: np.ndarray, tol: float = 1e-5, report: dict | None = None):
     """Replays a traced replica move by move.  For every move the FP32 dE the
     kernel decided on is compared with the FP64 difference of full energies
-    (the chain's form) on the same FP32-stored amplitudes.  Returns
-    (max |dE32-dE64| / sum|terms|, max plain relative error, n_moves)."""
+    (the chain's form, g2 over i<j) on the same FP32-stored amplitudes.
+    Returns (max |dE32-dE64| / sum|terms|, max plain relative error
+    |dE32-dE64| / |dE64|, n_moves).
+
+    When `report` is a dict it also receives the plain relative error's
+    median and the hamiltonian.cu form (hamiltonian.cu:30-38, g2 over i<=j):
+    the largest diagonal change |g_ii d|a_i|^2 + g_jj d|a_j|^2| of a move
+    relative to sum|terms| ("diag_max"), i.e. how far that form's dE is from
+    the chain's, and the largest error of dE32 + that diagonal change against
+    the FP64 difference of hamiltonian.cu-form energies ("ham_err_max")."""
     s = np.array(spins0, np.complex128)
     worst, worst_rel = 0.0, 0.0
+    rels, diag_max, ham_err = [], 0.0, 0.0
+    e_cur = None                   # energies of the current state (the last move's old or new)
+    g2d = None
+    if report is not None and isinstance(ref, DenseInit):
+        N = len(s)
+        g2c = np.ascontiguousarray(ref.g2, np.float64)
+        g2d = g2c.reshape(N, N, 2)[np.arange(N), np.arange(N), 0]
     for rec in trace:
         i0, j0 = int(rec["i0"]), int(rec["j0"])
         ai_old = complex(rec["ai_old"][0], rec["ai_old"][1])
@@ -219,16 +267,33 @@ def check_trace(ref, spins0: np.ndarray, trace: np.ndarray, tol: float = 1e-5):
         new = s.copy()
         new[i0] = complex(rec["ai_new"][0], rec["ai_new"][1])
         new[j0] = complex(rec["aj_new"][0], rec["aj_new"][1])
-        e_old = sum(ref.energy(s))
-        e_new = sum(ref.energy(new))
-        d64 = e_new - e_old
+        e2o, e4o = e_cur if e_cur is not None else ref.energy(s)
+        e2n, e4n = ref.energy(new)
+        d64 = (e2n + e4n) - (e2o + e4o)
         scale = ref.abs_terms(s, new, i0, j0)
         err = abs(float(rec["dE"]) - d64)
         worst = max(worst, err / scale if scale > 0 else err)
         if d64 != 0.0:
             worst_rel = max(worst_rel, err / abs(d64))
+            rels.append(err / abs(d64))
+        if g2d is not None:
+            # hamiltonian.cu form, computed on its own (g2 over i <= j, hamiltonian.cu:30-38)
+            hs = [lib().orc_energy_h2_with_diag(len(s), P(g2c), P(np.ascontiguousarray(
+                np.stack([v.real, v.imag], -1).ravel()))) for v in (s, new)]
+            d_ham = (hs[1] + e4n) - (hs[0] + e4o)
+            dd = sum(-g2d[k] * (abs(new[k]) ** 2 - abs(s[k]) ** 2) for k in (i0, j0))   # its diagonal part
+            diag_max = max(diag_max, abs(d_ham - d64) / scale if scale > 0 else abs(d_ham - d64))
+            ham_err = max(ham_err, abs(float(rec["dE"]) + dd - d_ham) / scale if scale > 0 else 0.0)
         if rec["accepted"]:
             s = new
+            e_cur = (e2n, e4n)
+        else:
+            e_cur = (e2o, e4o)
+    if report is not None:
+        report.update(n=len(trace), worst=worst, rel_max=worst_rel,
+                      rel_median=float(np.median(rels)) if rels else 0.0,
+                      diag_max=diag_max if g2d is not None else None,
+                      ham_err_max=ham_err if g2d is not None else None)
     return worst, worst_rel, len(trace)
 
 

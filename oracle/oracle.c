@@ -377,17 +377,26 @@ void orc_energy_dense(int N, const double* g2, const double* g4, const uint8_t* 
                 cplx prod = cm(g, cm(ld(sp, i), cj(ld(sp, j))));
                 s2 += -prod.x;
             }
-    int64_t nq = orc_n_quartets(N);
-    #pragma omp parallel for reduction(+:s4) schedule(static)
-    for (int64_t q = 0; q < nq; q++) {
-        cplx gq = { g4[2 * q], g4[2 * q + 1] };
-        uint8_t m = mask[q];
-        if ((gq.x == 0.0 && gq.y == 0.0) || m == 0) continue;
-        int i, j, k, l;
-        orc_decode_quartet(q, &i, &j, &k, &l);
-        for (int ch = 0; ch < 3; ch++)
-            if (m & (1 << ch)) s4 += quartet_term(gq, ch, ld(sp, i), ld(sp, j), ld(sp, k), ld(sp, l));
+    /* quartets in q order (q = C(l,4)+C(k,3)+C(j,2)+i, i fastest), one
+       partial sum per l, added in l order: deterministic for any thread count */
+    double* part = (double*)calloc((size_t)(N > 0 ? N : 1), sizeof(double));
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int l = 3; l < N; l++) {
+        double t = 0.0;
+        int64_t q = orc_n_quartets(l);
+        for (int k = 2; k < l; k++)
+            for (int j = 1; j < k; j++)
+                for (int i = 0; i < j; i++, q++) {
+                    cplx gq = { g4[2 * q], g4[2 * q + 1] };
+                    uint8_t m = mask[q];
+                    if ((gq.x == 0.0 && gq.y == 0.0) || m == 0) continue;
+                    for (int ch = 0; ch < 3; ch++)
+                        if (m & (1 << ch)) t += quartet_term(gq, ch, ld(sp, i), ld(sp, j), ld(sp, k), ld(sp, l));
+                }
+        part[l] = t;
     }
+    for (int l = 3; l < N; l++) s4 += part[l];
+    free(part);
     if (e2) *e2 = s2;
     if (e4) *e4 = s4;
 }
@@ -438,20 +447,24 @@ static double abs_h2(int N, const double* g2, const double* so, const double* sn
 double orc_dense_abs_terms(int N, const double* g2, const double* g4, const uint8_t* mask,
                            int h2_active, const double* so, const double* sn, int i0, int j0) {
     double s = h2_active ? abs_h2(N, g2, so, sn, i0, j0) : 0.0;
-    int64_t nq = orc_n_quartets(N);
-    for (int64_t q = 0; q < nq; q++) {
-        uint8_t m = mask[q];
-        cplx gq = { g4[2 * q], g4[2 * q + 1] };
-        if ((gq.x == 0.0 && gq.y == 0.0) || m == 0) continue;
-        int i, j, k, l;
-        orc_decode_quartet(q, &i, &j, &k, &l);
-        if (i != i0 && j != i0 && k != i0 && l != i0 && i != j0 && j != j0 && k != j0 && l != j0) continue;
-        for (int ch = 0; ch < 3; ch++)
-            if (m & (1 << ch)) {
-                s += fabs(quartet_term(gq, ch, ld(so, i), ld(so, j), ld(so, k), ld(so, l)));
-                s += fabs(quartet_term(gq, ch, ld(sn, i), ld(sn, j), ld(sn, k), ld(sn, l)));
+    /* quartets in q order; only those holding i0 or j0 contribute */
+    int64_t q = 0;
+    for (int l = 3; l < N; l++)
+        for (int k = 2; k < l; k++)
+            for (int j = 1; j < k; j++) {
+                const int hit_jkl = (j == i0 || j == j0 || k == i0 || k == j0 || l == i0 || l == j0);
+                for (int i = 0; i < j; i++, q++) {
+                    if (!hit_jkl && i != i0 && i != j0) continue;
+                    uint8_t m = mask[q];
+                    cplx gq = { g4[2 * q], g4[2 * q + 1] };
+                    if ((gq.x == 0.0 && gq.y == 0.0) || m == 0) continue;
+                    for (int ch = 0; ch < 3; ch++)
+                        if (m & (1 << ch)) {
+                            s += fabs(quartet_term(gq, ch, ld(so, i), ld(so, j), ld(so, k), ld(so, l)));
+                            s += fabs(quartet_term(gq, ch, ld(sn, i), ld(sn, j), ld(sn, k), ld(sn, l)));
+                        }
+                }
             }
-    }
     return s;
 }
 

@@ -67,3 +67,57 @@ def test_checkpoint_rejects_other_handles(ps, tmp_path):
     with _engine(ps) as b:
         with pytest.raises(ps.PspinError):
             b.checkpoint_load(str(tmp_path / "missing.bin"))
+
+
+def test_truncated_checkpoint_leaves_the_handle_unchanged(ps, tmp_path):
+    """The whole file is read and checked before anything is written."""
+    path = str(tmp_path / "ck.bin")
+    T, beta = ps.temperature_schedule(NT, 0.3, 1.5, True)
+    with _engine(ps) as a:
+        a.pt_init(NT, NR, beta, 1)
+        a.pt_run(9)
+        a.checkpoint_save(path)
+    raw = open(path, "rb").read()
+    for cut in (len(raw) - 8, len(raw) // 2, 200):
+        bad = str(tmp_path / f"cut{cut}.bin")
+        open(bad, "wb").write(raw[:cut])
+        with _engine(ps) as b:
+            b.pt_init(NT, NR, beta, 1)
+            b.pt_run(5)
+            before = _state(b)
+            with pytest.raises(ps.PspinError):
+                b.checkpoint_load(bad)
+            _same(before, _state(b))
+    longer = str(tmp_path / "long.bin")
+    open(longer, "wb").write(raw + b"\0")
+    with _engine(ps) as b:
+        with pytest.raises(ps.PspinError):
+            b.checkpoint_load(longer)
+
+
+def test_checkpoint_without_pt_drops_the_handles_pt_state(ps, tmp_path):
+    """A chain saved before any PT set-up, loaded into a handle that has PT
+    state, continues as the saved chain: plain sweeps equal, and the PT
+    state is gone (pspin_pt_run needs a new pspin_pt_init)."""
+    path = str(tmp_path / "ck.bin")
+    T, beta = ps.temperature_schedule(NT, 0.3, 1.5, True)
+    with _engine(ps) as a:
+        a.fill_betas(1.1)
+        a.sweep(7)
+        a.checkpoint_save(path)
+        a.sweep(11)
+        E_a, acc_a, _ = a.get_results()
+        s_a = a.get_spins()
+    with _engine(ps) as b:
+        b.pt_init(NT, NR, beta, 1)
+        b.pt_run(3)
+        b.checkpoint_load(path)
+        with pytest.raises(ps.PspinError):
+            b.pt_run(1)
+        b.sweep(11)
+        E_b, acc_b, _ = b.get_results()
+        s_b = b.get_spins()
+    np.testing.assert_array_equal(E_a, E_b)
+    np.testing.assert_array_equal(acc_a, acc_b)
+    for x, y in zip(s_a, s_b):
+        np.testing.assert_array_equal(x, y)

@@ -1,9 +1,8 @@
 """The allocation-free survivor count, pspin_fmc_survivors_static.
 
-Callers that cannot allocate device memory (work captured into a CUDA graph,
-hosts whose own pool owns all device memory, plugins handed only device
-pointers) get the FMC survivor count through this entry point, whose scratch
-is a static device array.  Its result must equal the existing entry point's
+Callers that cannot allocate device memory (hosts whose own pool owns all
+device memory, plugins handed only device pointers) get the FMC survivor
+count through this entry point, whose scratch is a static device array.  Its result must equal the existing entry point's
 (pspin_fmc_mask: the popcount of the mask it builds, and the per-channel
 counts read off that mask), on two calls in a row since the calls share the
 array.  Collected last so that a failure here leaves every other test run.
@@ -28,7 +27,8 @@ def _static_counts(ps, torch, N, w, gamma):
 
 
 @pytest.mark.parametrize("N,fmc,seed,gamma", [(10, 1, 0, 1.0), (32, 2, 42, 0.1), (64, 2, 42, 0.1),
-                                              (24, 2, 9, 1.0 / 46), (48, 1, 0, 2.0)])
+                                              (24, 2, 9, 1.0 / 46), (48, 1, 0, 2.0), (128, 2, 7, 0.05),
+                                              (256, 1, 0, 1.0)])
 def test_static_count_matches_existing_entry_point(ps, orc, N, fmc, seed, gamma):
     torch = pytest.importorskip("torch")
     w = orc.omega(N, fmc, seed)
