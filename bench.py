@@ -145,6 +145,10 @@ def run_engine(args, rank, world, device, dist):
     sps = args.sweeps_per_step
     moves_per_sweep = sum(NT * NREP_T * (N // 2) for N in Ns)
     flops_per_sweep = sum(NT * NREP_T * (N // 2) * flops_per_move(N) for N in Ns)
+    # the library's counts: the same algorithmic F (from the samples' masks)
+    # and the FP32 operations its field kernels execute on these site lists
+    alg_flops, exec_flops = eng.sweep_work()
+    assert abs(alg_flops - flops_per_sweep) <= 1e-9 * flops_per_sweep, (alg_flops, flops_per_sweep)
     entries = sum(eng.info(k).site_entries for k in range(len(Ns)))
 
     # ---- device-resident PT (value) -------------------------------------------
@@ -206,12 +210,32 @@ def run_engine(args, rank, world, device, dist):
             traffic = None if tuned_c == 0 else rec.get("bytes_per_launch")
         except Exception:
             traffic = None
-    executed = None   # executed FP32 ops per launch: 4 per data entry and replica + group/proposal overhead
+    executed = exec_flops * sweeps_per_launch / (per_launch_ms * 1e-3) / 1e12
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": "FMA-loop probe on this GPU (pspin_fp32_peak)",
             "kernel_ms_per_launch": per_launch_ms,
             "flops_per_launch": flops_per_sweep,
+            "executed_flops_per_launch": exec_flops * sweeps_per_launch,
+            "executed_achieved": executed, "executed_frac": executed / peak,
+            "note": "achieved/frac count the reference method's F = 20 W4 + 4 W2 + 64 FLOPs per pair-move; "
+                    "the local-field kernels execute about 4 per quartet term and replica "
+                    "(executed_*, counted from the site lists by pspin_sweep_work)",
             "site_entries": entries}
+
+    # ---- FP64 resync (every 1024 sweeps): its cost, amortised over its period
+    eng.set_profiling(False)
+    ev_r0 = torch.cuda.Event(enable_timing=True)
+    ev_r1 = torch.cuda.Event(enable_timing=True)
+    eng.resync()                       # warm
+    ev_r0.record(ext)
+    for _ in range(3):
+        eng.resync()
+    ev_r1.record(ext)
+    torch.cuda.synchronize(device)
+    resync_ms = ev_r0.elapsed_time(ev_r1) / 3
+    sweep_ms = ms / (args.steps * sps)
+    resync = {"ms": resync_ms, "every_sweeps": 1024, "share_of_loop": resync_ms / (resync_ms + 1024 * sweep_ms),
+              "value_with_resync": moves_per_sweep * world / ((sweep_ms + resync_ms / 1024) * 1e-3)}
 
     # ---- end to end: the reference's driver loop through the C ABI -------------------
     R_tot = eng.n_replicas
@@ -276,8 +300,15 @@ def run_engine(args, rank, world, device, dist):
                                    "chosen_by": "--shape" if shape else "pspin_autotune (2 sweeps per shape)"},
                    "launch": "sweep + exchange per PT step, replayed as CUDA graphs of 32 steps",
                    "setup_s": t_setup},
-        "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "resync": resync,
     }
+    # whole 2^14-sweep job of this workload from the measured parts: set-up,
+    # the e2e per-sweep loop, and a resync every 1024 sweeps
+    job_sweeps = 1 << 14
+    job_s = t_setup + job_sweeps * (e2e_s / (args.steps * sps)) + (job_sweeps // 1024) * resync_ms * 1e-3
+    out["e2e"]["job_projection"] = {"sweeps": job_sweeps, "seconds": job_s,
+                                    "pair_moves_per_s": moves_per_sweep * job_sweeps / job_s,
+                                    "parts": "set-up + 2^14 x (e2e seconds per sweep) + 16 resyncs"}
     return out
 
 

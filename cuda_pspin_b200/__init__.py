@@ -123,6 +123,7 @@ def load_library() -> ctypes.CDLL:
         "pspin_quartet_roundtrip": (ctypes.c_int, [ctypes.c_int, vp]),
         "pspin_fmc_survivors_static": (ctypes.c_int, [ctypes.c_int, vp, ctypes.c_double, vp, vp]),
         "pspin_local_fields": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp, vp]),
+        "pspin_sweep_work": (ctypes.c_int, [vp, vp, vp]),
         "pspin_set_proposal": (ctypes.c_int, [vp, ctypes.c_int]),
         "pspin_observe_init": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
         "pspin_autotune": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp]),
@@ -427,6 +428,13 @@ class Engine:
         return loss.value, g
 
     # -- measurement -------------------------------------------------------------
+    def sweep_work(self):
+        """(algorithmic, executed) FP32 operations of one sweep of every
+        sample and replica (pspin_sweep_work)."""
+        a, e = ctypes.c_double(), ctypes.c_double()
+        _check(self._lib.pspin_sweep_work(self._h, ctypes.byref(a), ctypes.byref(e)))
+        return a.value, e.value
+
     def stream_ptr(self) -> int:
         return int(self._lib.pspin_stream(self._h) or 0)
 

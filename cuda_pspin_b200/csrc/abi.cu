@@ -129,6 +129,7 @@ struct SampleHost {
     std::vector<int32_t> sq;         // sparse: [n][5]
     std::vector<double> sqg;
     int64_t site_entries = 0;
+    double exec_flops_lists = 0.0;   // FP32 ops per replica to accumulate all N site lists once
     int64_t g4_off = -1;             // dense: into d_g4re / d_mask
     int fc_tiles = 0;                // site lists are fully connected tiles
     int64_t nq_dense = 0;
@@ -866,6 +867,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         build_q64(qsv[k], q64[k]);
         std::vector<QuartetRec>().swap(qsv[k]);
         h.site_entries = (int64_t)lists[k].entries.size();
+        h.exec_flops_lists = list_exec_flops(lists[k], N, fc);
     }
 
     const auto t_p3 = clk();
@@ -1451,6 +1453,37 @@ extern "C" int pspin_get_info(pspin_state* s, int sample, pspin_info* info) {
     info->n_pairs_active = h.n_pairs_active;
     info->n_quart_active = h.n_quart_active;
     info->site_entries = h.site_entries;
+    return PSPIN_OK;
+}
+
+// Work of one sweep of every sample and replica.  Algorithmic: the
+// reference's per-move operation count F = 20 W4 + 4 W2 + 64 (a quartet term
+// as a 4-factor complex product times the coupling plus the accumulate, an
+// H2 term as one complex FMA pair, 64 for proposal and decision) with
+// W4 = A (8/N - 12/(N(N-1))) and W2 = P (4/N - 2/(N(N-1))) the expected
+// active quartets and off-diagonal pairs touching a uniformly random pair
+// (A = active quartet-channel pairs, P = active off-diagonal g2 pairs).
+// Executed: what the field kernels run -- per replica the operations of
+// accumulating the lists of the move's two sites (14 per group header and 4
+// per data entry; 56 per tile header and 16 per tile row), whose expectation
+// over a sweep's N/2 uniformly random pairs is one pass over all N lists,
+// plus the same 64 per move for proposal and decision.
+extern "C" int pspin_sweep_work(pspin_state* s, double* algorithmic_flops, double* executed_flops) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    double alg = 0.0, ex = 0.0;
+    for (const SampleHost& h : s->hs) {
+        const double N = h.N, R = h.R, moves = R * (double)(h.N / 2);
+        // active quartet-channel pairs: the mask's survivors (dense) or the
+        // selected quartets (sparse)
+        const double A = s->variant == PSPIN_SPARSE ? (double)h.sqg.size() : (double)h.n_quart_active;
+        const double P = h.h2_active ? (double)(h.n_pairs_active - h.N) : 0.0;   // the count includes the diagonal
+        const double W4 = A * (8.0 / N - 12.0 / (N * (N - 1.0)));
+        const double W2 = P * (4.0 / N - 2.0 / (N * (N - 1.0)));
+        alg += moves * (20.0 * W4 + 4.0 * W2 + 64.0);
+        ex += R * h.exec_flops_lists + moves * 64.0;
+    }
+    if (algorithmic_flops) *algorithmic_flops = alg;
+    if (executed_flops) *executed_flops = ex;
     return PSPIN_OK;
 }
 

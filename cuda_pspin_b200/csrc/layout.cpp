@@ -250,6 +250,39 @@ void build_site_tiles_fc(int N, const double* g2re, int h2_active, const double*
     }
 }
 
+// Per record, per replica: the group format costs 14 operations per header
+// (a_p conj(a_o1): 2 FMA + 2 MUL; the field update: 4 FMA) and 4 per data
+// entry (2 FMA); a fully connected tile costs 56 per header (4 partners x 14)
+// and 16 per row (8 FMA: 4 couplings times one gathered amplitude).
+double list_exec_flops(const SiteLists& L, int N, bool tiles) {
+    double total = 0.0;
+    const int64_t nchunks = (int64_t)L.chunk_start.size();
+    for (int m = 0; m < N; m++) {
+        const int c0 = L.site_chunks[(size_t)m * (kSplit + 1)];
+        const int c1 = L.site_chunks[(size_t)m * (kSplit + 1) + kSplit];
+        for (int c = c0; c < c1; c++) {
+            const int64_t b = L.chunk_start[c];
+            const int64_t e = (c + 1 < nchunks) ? L.chunk_start[c + 1] : (int64_t)L.entries.size();
+            const int2* R = L.entries.data() + b;
+            const int64_t n = e - b;
+            if (tiles) {
+                for (int64_t u = 0; u < n / 2;) {
+                    const int lo = R[2 * u].x >> 16, hi = R[2 * u].y;
+                    total += 56.0 + 16.0 * (hi - lo);
+                    u += 1 + (hi - lo);
+                }
+            } else {
+                for (int64_t u = 0; u < n;) {
+                    const int len = R[u].x;
+                    total += 14.0 + 4.0 * len;
+                    u += len + 1;
+                }
+            }
+        }
+    }
+    return total;
+}
+
 void build_q64(const std::vector<QuartetRec>& qs, std::vector<Q64>& out) {
     out.resize(qs.size());
     for (size_t t = 0; t < qs.size(); t++) {

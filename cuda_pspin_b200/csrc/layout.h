@@ -29,6 +29,11 @@ void build_pair_lists(int N, const double* g2re, int h2_active, const std::vecto
 // fully connected tiles from the dense g4 (channel 0 everywhere) and g2
 void build_site_tiles_fc(int N, const double* g2re, int h2_active, const double* g4re, SiteLists& out);
 void build_q64(const std::vector<QuartetRec>& qs, std::vector<Q64>& out);
+// FP32 operations the sweep kernels execute, per replica, to accumulate the
+// lists of all N sites once (the expected work of one sweep's N/2 moves over
+// their two sites each), walking the packed chunks exactly as
+// accumulate_chunk / accumulate_tiles do (padding words included).
+double list_exec_flops(const SiteLists& L, int N, bool tiles);
 // every active (q, ch) of a dense mask in q order
 void dense_quartets(int N, const double* g4re, const uint8_t* mask, std::vector<QuartetRec>& out);
 

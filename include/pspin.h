@@ -316,6 +316,14 @@ void* pspin_stream(pspin_state* s);
 int  pspin_set_profiling(pspin_state* s, int on);
 int  pspin_get_profile(pspin_state* s, double* sweep_kernel_ms, int64_t* sweep_launches,
                        int64_t* kernel_launches);
+/* Work of one sweep of all samples and replicas (no reference
+ * counterpart): algorithmic_flops by the reference method's count per
+ * pair-move, F = 20 W4 + 4 W2 + 64 (W4, W2: expected active quartets and
+ * off-diagonal pairs touching a random pair), and executed_flops, the FP32
+ * operations the local-field kernels actually run on this handle's site
+ * lists (about 4 per quartet term and replica) plus the same 64 per move.
+ * Either pointer may be NULL. */
+int  pspin_sweep_work(pspin_state* s, double* algorithmic_flops, double* executed_flops);
 /* FP32 FMA throughput of the current device (TFLOP/s), measured by a
  * register-resident FMA loop over all SMs: the roofline denominator of the
  * FP32 sweep. */
