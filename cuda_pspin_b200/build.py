@@ -133,7 +133,7 @@ def build_ref() -> None:
         return
     if shutil.which("make") is None:
         return
-    _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", f"PSPIN_REF={ref}"])
+    _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "compat", f"PSPIN_REF={ref}"])
 
 
 def main(argv: list[str] | None = None) -> int:

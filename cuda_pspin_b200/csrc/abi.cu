@@ -1487,6 +1487,17 @@ extern "C" int pspin_sweep_work(pspin_state* s, double* algorithmic_flops, doubl
     return PSPIN_OK;
 }
 
+extern "C" int pspin_device_arrays(pspin_state* s, int64_t** accepted, int64_t** proposed, double** energies,
+                                   double** betas) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    static_assert(sizeof(long long) == sizeof(int64_t), "counter width");
+    if (accepted) *accepted = reinterpret_cast<int64_t*>(s->d_acc);
+    if (proposed) *proposed = reinterpret_cast<int64_t*>(s->d_prop);
+    if (energies) *energies = s->d_E;
+    if (betas) *betas = s->d_beta;
+    return PSPIN_OK;
+}
+
 extern "C" int pspin_get_omega(pspin_state* s, int sample, double* omega) {
     if (!s || !omega || sample < 0 || sample >= s->S) return fail(PSPIN_ERR_ARG, "bad arguments");
     const SampleHost& h = s->hs[sample];

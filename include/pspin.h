@@ -162,6 +162,18 @@ int  pspin_resync(pspin_state* s);   /* FP64 energy recompute + constraint renor
 int  pspin_total_replicas(const pspin_state* s);
 int  pspin_num_samples(const pspin_state* s);
 
+/* Device pointers into the handle's own per-replica arrays, which the
+ * reference's MCState exposes as fields (d_accepted, d_proposed,
+ * d_energies, d_betas; mc.h:9-30): int64 accepted and proposed counters,
+ * FP64 running energies and betas, [total replicas] each, physical replica
+ * order.  Valid until pspin_destroy.  The handle works on its own stream,
+ * which does not wait for other streams: work a caller enqueues on these
+ * arrays (the reference's drivers cudaMemset the counters,
+ * parallel_tempering.cu:396-397) must be complete before the next call on
+ * the handle.  Any output pointer may be NULL. */
+int  pspin_device_arrays(pspin_state* s, int64_t** accepted, int64_t** proposed, double** energies,
+                         double** betas);
+
 /* ---- disorder introspection (MCState fields read by the drivers) ---- */
 int  pspin_get_info(pspin_state* s, int sample, pspin_info* info);
 int  pspin_get_omega(pspin_state* s, int sample, double* omega); /* [N]; ERR_STATE if FC */
