@@ -160,6 +160,7 @@ struct pspin_state {
     int64_t* d_chunk_start = nullptr;
     int* d_site_chunks = nullptr;
     int* d_pair_chunks = nullptr;       // pair sub-lists, built on the first two-pass proposal
+    uint32_t* d_nbmask = nullptr;       // per sample: neighbour masks (rows of ceil(N/32) words)
     int64_t ent_total = 0, chunk_total = 0;
     Q64* d_q64 = nullptr;
     double* d_g2 = nullptr;
@@ -234,7 +235,7 @@ static void free_state(pspin_state* s) {
                     s->d_beta_sched, s->d_perm, s->d_drand, s->d_ex_acc, s->d_ex_prop, s->d_trace,
                     s->d_tc_w, s->d_tc_x, s->d_tc_f, s->d_tc_ws, s->d_tc_h, s->d_f64_h, s->d_tc_e,
                     s->d_w32, s->d_adam_m, s->d_adam_v, s->d_grad, s->d_wbf, s->d_records, s->d_rec_count,
-                    s->d_save, s->d_loss, s->d_idx, s->d_obs_E, s->d_obs_q, s->d_pair_chunks};
+                    s->d_save, s->d_loss, s->d_idx, s->d_obs_E, s->d_obs_q, s->d_pair_chunks, s->d_nbmask};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& e : s->ev_pool) {
@@ -873,6 +874,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     const auto t_p3 = clk();
     // ---- concatenate and upload
     int64_t ent_total = 0, split_total = 0, q_total = 0, g2_total = 0, spin_off = 0, rep_off = 0, chunk_total = 0;
+    int64_t nb_total = 0;
     s->sd.resize(n);
     for (int k = 0; k < n; k++) {
         SampleHost& h = s->hs[k];
@@ -890,6 +892,8 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         d.nq = (int64_t)q64[k].size();
         d.g2_off = g2_total;
         d.pair_off = -1;
+        d.nb_off = nb_total;
+        nb_total += (int64_t)h.N * ((h.N + 31) / 32);
         uint64_t pk = h.cfg.seed + 7000;
         const uint64_t key = splitmix64(pk);
         d.pair_key0 = (uint32_t)key;
@@ -907,6 +911,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     std::vector<int> site_chunks(split_total);
     std::vector<int64_t> chunk_start(chunk_total + 1);
     std::vector<Q64> qall(q_total);
+    std::vector<uint32_t> nball(nb_total, 0u);
     std::vector<double> g2all(g2_total);
     std::vector<float2> spall(s->spin_total);
     std::vector<double> tall(s->R_tot), Eall(s->R_tot, 0.0);
@@ -922,6 +927,21 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
             eoff += (int64_t)lists[k].entries.size();
             coff += (int64_t)lists[k].chunk_start.size();
             std::copy(q64[k].begin(), q64[k].end(), qall.begin() + d.q_off);
+            {   // neighbour masks: sites that share an active quartet, or any g2 term, with m
+                const int Nk = d.N, wpr = (Nk + 31) / 32;
+                uint32_t* rows = nball.data() + d.nb_off;
+                auto set = [&](int a, int b) { rows[(size_t)a * wpr + b / 32] |= 1u << (b % 32); };
+                for (const Q64& q : q64[k]) {
+                    const int v[4] = {q.i, q.j, q.k, q.lch & 0x3FFF};
+                    for (int a = 0; a < 4; a++)
+                        for (int b = 0; b < 4; b++)
+                            if (a != b) set(v[a], v[b]);
+                }
+                if (d.h2_active)
+                    for (int a = 0; a < Nk; a++)
+                        for (int b = 0; b < Nk; b++)
+                            if (a != b) set(a, b);
+            }
             std::copy(s->hs[k].g2re.begin(), s->hs[k].g2re.end(), g2all.begin() + d.g2_off);
             std::copy(spins[k].begin(), spins[k].end(), spall.begin() + d.spin_off);
             std::copy(targets[k].begin(), targets[k].end(), tall.begin() + d.rep_off);
@@ -949,10 +969,11 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         const int c = s->opt.cluster_size == 0 ? 1 : s->opt.cluster_size;
         s->warps2 = s->warps;
         if (c == -1) {
-            if (resident_smem_bytes_host(s->max_N, s->max_site_entries) > 227 * 1024)
+            const int rw = s->opt.warps_per_unit > 0 ? s->opt.warps_per_unit : 1;
+            if (resident_smem_bytes_host(s->max_N, s->max_site_entries, rw) > 227 * 1024)
                 return bail(fail(PSPIN_ERR_ARG, "the site lists do not fit in shared memory (cluster_size -1)"));
             s->cluster = 0;
-            s->warps = 1;
+            s->warps = rw;
         } else {
             if (c != 1 && c != 2 && c != 4 && c != 8 && c != 16)
                 return bail(fail(PSPIN_ERR_ARG, "cluster_size must be -1, 1, 2, 4, 8 or 16"));
@@ -974,6 +995,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         (rc = dalloc(&s->d_chunk_start, (size_t)chunk_total + 1)) ||
         (rc = dalloc(&s->d_q64, (size_t)std::max<int64_t>(q_total, 1))) ||
         (rc = dalloc(&s->d_g2, (size_t)g2_total)) || (rc = dalloc(&s->d_sweep_counter, 1)) ||
+        (rc = dalloc(&s->d_nbmask, (size_t)std::max<int64_t>(nb_total, 1))) ||
         (rc = dalloc(&s->d_status, 1)))
         return bail(rc);
     auto up = [&](void* dst, const void* src, size_t bytes) -> int {
@@ -995,6 +1017,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         (rc = up(s->d_chunk_start, chunk_start.data(), chunk_start.size() * sizeof(int64_t))) ||
         (rc = up(s->d_q64, qall.data(), qall.size() * sizeof(Q64))) ||
         (rc = up(s->d_g2, g2all.data(), g2all.size() * sizeof(double))) ||
+        (rc = up(s->d_nbmask, nball.data(), nball.size() * sizeof(uint32_t))) ||
         (rc = up(s->d_beta, ones.data(), ones.size() * sizeof(double))))
         return bail(rc);
     {
@@ -1056,6 +1079,7 @@ static int enqueue_step(pspin_state* s, int nsweeps, bool exchange, cudaEvent_t 
     p.chunk_start = s->d_chunk_start;
     p.site_chunks = s->d_site_chunks;
     p.pair_chunks = s->d_pair_chunks;
+    p.nbmask = s->d_nbmask;
     p.sweep_counter = s->d_sweep_counter;
     p.nsweeps = nsweeps;
     p.warps = s->proposal == PSPIN_PROPOSAL_PLAIN ? s->warps : s->warps2;
@@ -1246,8 +1270,8 @@ static int run_sweeps(pspin_state* s, int nsweeps, bool pt) {
 // memory, co-residency of the cluster); the plain kernel for cluster 1.
 static bool shape_fits(pspin_state* s, int warps, int cluster) {
     if (cluster == 0)
-        return s->proposal == PSPIN_PROPOSAL_PLAIN && warps == 1 &&
-               resident_smem_bytes_host(s->max_N, s->max_site_entries) <= 227 * 1024;
+        return s->proposal == PSPIN_PROPOSAL_PLAIN &&
+               resident_smem_bytes_host(s->max_N, s->max_site_entries, warps) <= 227 * 1024;
     if (cluster * warps > kSplit) return false;
     if (s->proposal != PSPIN_PROPOSAL_PLAIN) {
         if (learned_smem_bytes_host(s->max_N, warps, cluster) > 227 * 1024) return false;

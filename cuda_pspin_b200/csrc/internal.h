@@ -75,6 +75,7 @@ struct SampleDev {
     int64_t nq;            // active (quartet, channel) pairs in the Q64 table
     int64_t g2_off;        // index into g2 (N*N doubles)
     int64_t pair_off;      // index into the pair sub-list chunks (N(N-1)*33 entries), -1: not built
+    int64_t nb_off;        // index into the neighbour masks (N rows of ceil(N/32) words)
     uint32_t pair_key0, pair_key1;
 };
 
@@ -103,6 +104,7 @@ struct SweepParams {
     const int64_t* chunk_start;
     const int* site_chunks;
     const int* pair_chunks;           // pair sub-lists (two-pass proposals), or null
+    const uint32_t* nbmask;           // per sample: row m = sites sharing a quartet (or a g2 term) with m
     const long long* sweep_counter;   // global sweep index at launch start
     int nsweeps;
     int warps;                        // warps per unit (divides 32)
@@ -131,9 +133,12 @@ cudaError_t launch_sweep(const SweepParams& p, int n_units, int variant, int max
 cudaError_t launch_sweep_cluster(const SweepParams& p, int n_units, int variant, int max_N, cudaStream_t st,
                                  int* max_clusters);
 size_t cluster_smem_bytes_host(int N, int warps, int C);
+// the list-resident kernel; warps > 1 runs batches of consecutive moves that
+// commute (no site of one in the other's quartet neighbourhood) on separate
+// warps, with the neighbour masks `nbmask`
 cudaError_t launch_sweep_resident(const SweepParams& p, int n_units, int variant, int max_N, int64_t max_entries,
                                   cudaStream_t st);
-size_t resident_smem_bytes_host(int N, int64_t entries);
+size_t resident_smem_bytes_host(int N, int64_t entries, int warps);
 
 struct EnergyParams {
     const SampleDev* samples;

@@ -1,36 +1,55 @@
 // sweep_cluster.cu -- the plain pair-rotation sweep with one replica block
-// split over a thread-block cluster of C CTAs (C = 2..16), for workloads
-// with fewer replica blocks than SMs (one large sample, few replicas).
+// split over a thread-block cluster of C CTAs (C = 2..16).
 //
 // Same moves, RNG streams and Metropolis rule as sweep_kernel.  Every CTA of
 // the cluster holds the block's amplitudes in its own shared memory and
-// reads 1/C of every site list through its own TMA rings.  Per move:
-//   1. each CTA sums its warps' partial fields and stores the float4 of
-//      every lane into slot [rank] of every CTA's exchange buffer
-//      (distributed shared memory, mapa + st.shared::cluster);
-//   2. one cluster barrier (release / acquire);
-//   3. warp 0 of every CTA adds the C partials in rank order -- the same
-//      numbers in the same order everywhere -- and takes the same Metropolis
-//      decision on the same random words, so the CTAs' amplitude copies stay
-//      identical without broadcasting them.
-// The exchange buffer is double-buffered by move parity: a CTA can be at
-// most one move ahead of another (it cannot pass the next cluster barrier
-// before the slower CTA has read the current buffer).  Rank 0 writes the
-// results back.
+// reads 1/C of every site list through its own TMA rings; the C*W warps of
+// the cluster each own kSplit/(C*W) of the 32 parts of a list.
+//
+// One barrier per move.  A move m is
+//   field pass m: every warp accumulates its share of the two sites' fields
+//      (with the proposed a_j in j's slot) and stores its float4 partial into
+//      slot [rank*W + warp] of every CTA's exchange buffer (distributed
+//      shared memory, mapa + st.shared::cluster); then one cluster barrier
+//      (release / acquire);
+//   decision m: EVERY warp of every CTA sums the C*W partials in the same
+//      order (per CTA its warps in order, then the CTAs in rank order) and
+//      takes the same Metropolis decision on the same random words, so no
+//      warp waits for another to decide or to broadcast;
+//   proposal m+1: every warp computes it from the state after the decision
+//      and writes the same final values into its lanes' amplitude slots --
+//      the decided amplitudes of move m's pair and the proposed a_j of move
+//      m+1 -- before its own field pass m+1 reads them.  All writes between
+//      two barriers carry the values of the state that the next field pass
+//      reads, and each lane reads only its own replica's column, so the
+//      warps need no barrier between deciding and reading.
+// The state-independent part of a proposal (random words, sines and
+// cosines) is computed one move ahead by the last warp of each CTA into a
+// buffer double-buffered by move parity, as is the exchange buffer: no warp
+// can be more than one move ahead of another (the barrier of each move
+// waits for all of them).  Rank 0 writes the results back.
 #include "sweep_common.cuh"
 #include "../../include/pspin.h"
 
 namespace pspin {
 
-// the exchange buffer follows the plain kernel's layout, rounded up to 16
-// bytes (float4 stores and loads; with one warp that layout ends at 8 mod 16)
+// Shared memory of one CTA: amplitudes [(N+1)][32] float2; TMA rings
+// [W][kStages][kStage] int2; ring mbarriers [W][kStages]; the precomputed
+// proposal parts [2][7][32] float; then, at a 16-byte boundary, the
+// exchange buffer [2][C*W][32] float4 and the cluster's abort flag.
+__host__ __device__ inline size_t cluster_pre_offset(int N, int warps) {
+    return (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)warps * kStages * kStage * sizeof(int2) +
+           (size_t)warps * kStages * sizeof(uint64_t);
+}
 __host__ __device__ inline size_t cluster_buffer_offset(int N, int warps) {
-    return (sweep_smem_bytes(N, warps) + 15) & ~(size_t)15;
+    return (cluster_pre_offset(N, warps) + (size_t)2 * 7 * kRepBlock * sizeof(float) + 15) & ~(size_t)15;
+}
+inline size_t cluster_smem_bytes(int N, int warps, int C) {
+    return cluster_buffer_offset(N, warps) + (size_t)2 * C * warps * kRepBlock * sizeof(float4) + 16;
 }
 
-// exchange buffer [2][C][32] float4, then the cluster's abort flag (one word)
-inline size_t cluster_smem_bytes(int N, int warps, int C) {
-    return cluster_buffer_offset(N, warps) + (size_t)2 * C * kRepBlock * sizeof(float4) + 16;
+__device__ __forceinline__ void add4(float4& a, const float4 b) {
+    a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
 }
 
 template <int VARIANT>
@@ -45,15 +64,16 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int W = P.warps;
+    const int CW = C * W;
+    const int helper = W - 1;                  // computes the proposal parts one move ahead
     float2* sp = reinterpret_cast<float2*>(smem_raw);                          // [(N+1)][32]
-    float4* red = reinterpret_cast<float4*>(sp + (size_t)(N + 1) * kRepBlock);  // [W][32]
-    int2* ring_all = reinterpret_cast<int2*>(red + (size_t)W * kRepBlock);
+    int2* ring_all = reinterpret_cast<int2*>(sp + (size_t)(N + 1) * kRepBlock);
     int2* ring = ring_all + (size_t)warp * kStages * kStage;
     uint64_t* bars_all = reinterpret_cast<uint64_t*>(ring_all + (size_t)W * kStages * kStage);
     uint64_t* bars = bars_all + warp * kStages;
-    float4* cred = reinterpret_cast<float4*>(smem_raw + cluster_buffer_offset(N, W));   // [2][C][32]
-    // raised in every CTA of the cluster by a CTA that aborts (see below)
-    int* cflag = reinterpret_cast<int*>(cred + (size_t)2 * C * kRepBlock);
+    float* pre = reinterpret_cast<float*>(smem_raw + cluster_pre_offset(N, W));        // [2][7][32]
+    float4* cred = reinterpret_cast<float4*>(smem_raw + cluster_buffer_offset(N, W));  // [2][C*W][32]
+    int* cflag = reinterpret_cast<int*>(cred + (size_t)2 * CW * kRepBlock);            // cluster abort flag
 
     const bool active = lane < U.rep_count;
     const bool writer = rank == 0;
@@ -68,22 +88,23 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     if (threadIdx.x < kRepBlock) sp[N * kRepBlock + threadIdx.x] = make_float2(1.f, 0.f);  // virtual site
     if (threadIdx.x == 0) *cflag = 0;
 
+    // every warp decides, so every warp holds its lanes' betas
     double E = 0.0, beta_d = 0.0;
     float beta = 0.f;
     long long nacc = 0, nprop = 0;
     uint32_t k0 = 0, k1 = 0;
-    if (warp == 0 && active) {
-        E = P.energy[gr];
+    if (active) {
         beta_d = P.beta[gr];
         beta = (float)beta_d;
         const uint64_t key = P.key[gr];
         k0 = (uint32_t)key;
         k1 = (uint32_t)(key >> 32);
+        if (warp == 0) E = P.energy[gr];
     }
     const long long sweep0 = *P.sweep_counter;
     const int steps = N / 2;
     const int total = P.nsweeps * steps;
-    const int TW = C * W, gw = (int)rank * W + warp;
+    const int gw = (int)rank * W + warp;
 
     Stream<2, false> st;
     st.key0 = S.pair_key0;
@@ -94,8 +115,8 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     st.sweep0 = sweep0;
     st.steps = steps;
     st.total = total;
-    st.part0 = gw * (kSplit / TW);
-    st.part1 = (gw + 1) * (kSplit / TW);
+    st.part0 = gw * (kSplit / CW);
+    st.part1 = (gw + 1) * (kSplit / CW);
 
     if (lane == 0) {
         for (int s = 0; s < kStages; s++) mbar_init(bars + s, 1);
@@ -120,19 +141,31 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     };
     for (int s = 0; s < kStages; s++) issue();
 
+    // the helper warp: random words, sines and cosines of move m into pre[m & 1]
+    auto make_pre = [&](int m) {
+        const long long sw = sweep0 + m / steps;
+        float t[7];
+        move_trig<VARIANT>(move_words(k0, k1, (uint64_t)sw, (uint32_t)(m % steps)), t);
+        float* dst = pre + (m & 1) * 7 * kRepBlock;
+#pragma unroll
+        for (int q = 0; q < 7; q++) dst[q * kRepBlock + lane] = t[q];
+    };
+    auto pair_of = [&](int m, int& i0, int& j0) {
+        pair_pick(S.pair_key0, S.pair_key1, (uint64_t)(sweep0 + m / steps), (uint32_t)(m % steps), N, i0, j0);
+    };
+    // the pending move (every warp): pair, current and proposed amplitudes, uniform
     int ci0 = 0, cj0 = 0;
     float2 cai = make_float2(0.f, 0.f), caj = cai, cain = cai, cajn = cai;
     float cu = 0.f;
-    auto prepare = [&](int m) {
-        const long long sw = sweep0 + m / steps;
-        const int k = m % steps;
-        pair_pick(S.pair_key0, S.pair_key1, (uint64_t)sw, (uint32_t)k, N, ci0, cj0);
-        cai = sp[ci0 * kRepBlock + lane];
-        caj = sp[cj0 * kRepBlock + lane];
-        const U4 w = move_words(k0, k1, (uint64_t)sw, (uint32_t)k);
-        propose<VARIANT>(cai, caj, w, cain, cajn);
-        cu = u01f(w.w);
-        sp[cj0 * kRepBlock + lane] = cajn;     // h_i is evaluated at the proposed a_j
+    auto take_pre = [&](int m, float2 ai, float2 aj) {
+        const float* src = pre + (m & 1) * 7 * kRepBlock;
+        float t[7];
+#pragma unroll
+        for (int q = 0; q < 7; q++) t[q] = src[q * kRepBlock + lane];
+        cai = ai;
+        caj = aj;
+        propose_with<VARIANT>(ai, aj, t, cain, cajn);
+        cu = t[6];
     };
 
     __shared__ __align__(8) uint64_t stall_bar;      // test hook: nothing arrives on it
@@ -140,15 +173,19 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
         mbar_init(&stall_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if (warp == helper && total > 0) make_pre(0);
     __syncthreads();
-    if (warp == 0 && total > 0) prepare(0);
-    __syncthreads();
+    if (total > 0) {
+        pair_of(0, ci0, cj0);
+        take_pre(0, sp[ci0 * kRepBlock + lane], sp[cj0 * kRepBlock + lane]);
+        sp[cj0 * kRepBlock + lane] = cajn;     // h_i is evaluated at the proposed a_j
+    }
     cluster_sync();                            // every CTA runs before the first remote store
 
     bool aborted = false;
     for (int m = 0; m < total; m++) {
-        const long long sw = sweep0 + m / steps;
-        const int k = m % steps;
+        if (warp == helper && m + 1 < total) make_pre(m + 1);
+        // ---- field pass m
         float h[4] = {0.f, 0.f, 0.f, 0.f};
         if (m == P.stall_move) ok = stall_wait(&stall_bar, P.status, P.wait_clocks);
         for (int which = 0; which < 2 && ok; which++) {
@@ -167,50 +204,55 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
                 issue();
             }
         }
-        red[warp * kRepBlock + lane] = make_float4(h[0], h[1], h[2], h[3]);
-        const bool bad = __syncthreads_or(!ok);
-        float4* buf = cred + (size_t)(m & 1) * C * kRepBlock;
-        if (warp == 0) {
-            float4 hs = red[lane];
-            for (int w = 1; w < W; w++) {
-                const float4 v = red[w * kRepBlock + lane];
-                hs.x += v.x; hs.y += v.y; hs.z += v.z; hs.w += v.w;
-            }
-            for (int q = 0; q < C; q++) st_cluster_f4(buf + rank * kRepBlock + lane, (uint32_t)q, hs);
-            // an aborting CTA raises the flag in every CTA before the barrier,
-            // so all of them read it after the same barrier and leave together
-            if (bad && lane == 0)
-                for (int q = 0; q < C; q++) st_cluster_u32(cflag, (uint32_t)q, 1u);
+        // the next move's pair and its sites' amplitudes in the state the
+        // field pass just read (this move's decision can change only ci0, cj0)
+        int ni0 = 0, nj0 = 0;
+        float2 nai = make_float2(0.f, 0.f), naj = nai;
+        if (m + 1 < total) {
+            pair_of(m + 1, ni0, nj0);
+            nai = sp[ni0 * kRepBlock + lane];
+            naj = sp[nj0 * kRepBlock + lane];
         }
+        // ---- partials to every CTA, one cluster barrier
+        float4* buf = cred + (size_t)(m & 1) * CW * kRepBlock;
+        const float4 mine = make_float4(h[0], h[1], h[2], h[3]);
+        for (int q = 0; q < C; q++) st_cluster_f4(buf + gw * kRepBlock + lane, (uint32_t)q, mine);
+        // a warp that aborts raises the flag in every CTA before the barrier,
+        // so all of them read it after the same barrier and leave together
+        if (!ok && lane == 0)
+            for (int q = 0; q < C; q++) st_cluster_u32(cflag, (uint32_t)q, 1u);
         cluster_sync();
         if (*(volatile int*)cflag) {
             aborted = true;
             break;
         }
 
+        // ---- decision m, the same in every warp
+        float4 hs = buf[lane];
+        for (int w = 1; w < W; w++) add4(hs, buf[w * kRepBlock + lane]);
+        for (int q = 1; q < C; q++) {
+            float4 part = buf[(q * W) * kRepBlock + lane];
+            for (int w = 1; w < W; w++) add4(part, buf[(q * W + w) * kRepBlock + lane]);
+            add4(hs, part);
+        }
+        const float dix = cain.x - cai.x, diy = cain.y - cai.y;
+        const float djx = cajn.x - caj.x, djy = cajn.y - caj.y;
+        const float dE = -fmaf(dix, hs.x, -diy * hs.y) - fmaf(djx, hs.z, -djy * hs.w);
+        // mc.cu:288-297: beta == 0 accepts everything; otherwise dE <= 0 or u < exp(-beta dE)
+        bool accept;
+        if (beta_d == 0.0) accept = true;
+        else accept = (dE <= 0.f) || (cu < expf(-beta * dE));
+        const float2 ai_post = accept ? cain : cai, aj_post = accept ? cajn : caj;
         if (warp == 0) {
-            float4 hs = buf[lane];
-            for (int q = 1; q < C; q++) {
-                const float4 v = buf[q * kRepBlock + lane];
-                hs.x += v.x; hs.y += v.y; hs.z += v.z; hs.w += v.w;
-            }
-            const float dix = cain.x - cai.x, diy = cain.y - cai.y;
-            const float djx = cajn.x - caj.x, djy = cajn.y - caj.y;
-            const float dE = -fmaf(dix, hs.x, -diy * hs.y) - fmaf(djx, hs.z, -djy * hs.w);
-            bool accept;
-            if (beta_d == 0.0) accept = true;
-            else accept = (dE <= 0.f) || (cu < expf(-beta * dE));
             if (accept) {
-                sp[ci0 * kRepBlock + lane] = cain;
                 E += (double)dE;
                 nacc++;
-            } else {
-                sp[cj0 * kRepBlock + lane] = caj;
             }
             nprop++;
             if (writer && P.trace != nullptr && U.sample == P.trace_sample && U.rep_begin + lane == P.trace_rep &&
                 active) {
-                const long long idx = (sw - P.trace_sweep0) * steps + k;
+                const long long sw = sweep0 + m / steps;
+                const long long idx = (sw - P.trace_sweep0) * steps + m % steps;
                 if (idx >= 0 && idx < P.trace_cap) {
                     pspin_move_record* rec = reinterpret_cast<pspin_move_record*>(P.trace) + idx;
                     rec->i0 = ci0; rec->j0 = cj0;
@@ -224,11 +266,25 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
                     rec->log_u = logf(cu);
                 }
             }
-            if (m + 1 < total) prepare(m + 1);
         }
-        __syncthreads();
+        // ---- proposal m+1 and the final values of the state it reads
+        if (m + 1 < total) {
+            const float2 ai1 = ni0 == ci0 ? ai_post : (ni0 == cj0 ? aj_post : nai);
+            const float2 aj1 = nj0 == ci0 ? ai_post : (nj0 == cj0 ? aj_post : naj);
+            const int pi0 = ci0, pj0 = cj0;
+            ci0 = ni0;
+            cj0 = nj0;
+            take_pre(m + 1, ai1, aj1);
+            sp[pi0 * kRepBlock + lane] = pi0 == cj0 ? cajn : ai_post;
+            sp[pj0 * kRepBlock + lane] = pj0 == cj0 ? cajn : aj_post;
+            sp[cj0 * kRepBlock + lane] = cajn;     // h_i of move m+1 is evaluated at its proposed a_j
+        } else {
+            sp[ci0 * kRepBlock + lane] = ai_post;
+            sp[cj0 * kRepBlock + lane] = aj_post;
+        }
     }
     if (aborted) drain_ring(bars, kStages, consumed, issued, P.status);   // state stays as before the launch
+    __syncthreads();                           // every warp's final writes before the write-back
     if (writer && !aborted) {
         for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
             const int site = idx >> 5, l = idx & 31;

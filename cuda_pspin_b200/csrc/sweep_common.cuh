@@ -7,17 +7,34 @@
 
 namespace pspin {
 
+// The state-independent part of a move's proposal, from its four random
+// words: t[0], t[1] = sin, cos of the rotation angle (sphere) or
+// sqrt(1-u), sqrt(u) of the transfer (cube); t[2..5] = sin, cos of the two
+// phases; t[6] = the Metropolis uniform.
 template <int VARIANT>
-__device__ __forceinline__ void propose(float2 ai, float2 aj, U4 w, float2& ain, float2& ajn) {
+__device__ __forceinline__ void move_trig(U4 w, float* t) {
+    if (VARIANT == 0) {
+        sincospif(2.0f * u01f(w.x), &t[0], &t[1]);
+    } else {
+        const float u = u01f_open0(w.x);
+        t[0] = sqrtf(1.0f - u);
+        t[1] = sqrtf(u);
+    }
+    sincospif(2.0f * u01f(w.y), &t[2], &t[3]);
+    sincospif(2.0f * u01f(w.z), &t[4], &t[5]);
+    t[6] = u01f(w.w);
+}
+
+// The state-dependent part: the proposed amplitudes from the current ones.
+template <int VARIANT>
+__device__ __forceinline__ void propose_with(float2 ai, float2 aj, const float* t, float2& ain, float2& ajn) {
+    const float s1 = t[2], c1 = t[3], s2 = t[4], c2 = t[5];
     if (VARIANT == 0) {
         // spins.h:17-52: a_i' = a_i e^{-i phi1} sqrt((r1+r2)/r1) cos(alpha),
         //                a_j' = a_j e^{-i phi2} sqrt((r1+r2)/r2) sin(alpha)
+        const float sa = t[0], ca = t[1];
         float r1 = fmaf(ai.x, ai.x, ai.y * ai.y);
         float r2 = fmaf(aj.x, aj.x, aj.y * aj.y);
-        float sa, ca, s1, c1, s2, c2;
-        sincospif(2.0f * u01f(w.x), &sa, &ca);
-        sincospif(2.0f * u01f(w.y), &s1, &c1);
-        sincospif(2.0f * u01f(w.z), &s2, &c2);
         float s = r1 + r2;
         float f1 = sqrtf(s / r1) * ca;
         float f2 = sqrtf(s / r2) * sa;
@@ -26,18 +43,21 @@ __device__ __forceinline__ void propose(float2 ai, float2 aj, U4 w, float2& ain,
     } else {
         // spins_sparse.h:26-56: |a_i'|^2 = sqrt(S4) sqrt(1-u), |a_j'|^2 = sqrt(S4) sqrt(u),
         // absolute phases phi1, phi2
-        float u = u01f_open0(w.x);
         float r1 = fmaf(ai.x, ai.x, ai.y * ai.y);
         float r2 = fmaf(aj.x, aj.x, aj.y * aj.y);
         float q = sqrtf(fmaf(r1, r1, r2 * r2));
-        float m1 = sqrtf(q * sqrtf(1.0f - u));
-        float m2 = sqrtf(q * sqrtf(u));
-        float s1, c1, s2, c2;
-        sincospif(2.0f * u01f(w.y), &s1, &c1);
-        sincospif(2.0f * u01f(w.z), &s2, &c2);
+        float m1 = sqrtf(q * t[0]);
+        float m2 = sqrtf(q * t[1]);
         ain = make_float2(m1 * c1, m1 * s1);
         ajn = make_float2(m2 * c2, m2 * s2);
     }
+}
+
+template <int VARIANT>
+__device__ __forceinline__ void propose(float2 ai, float2 aj, U4 w, float2& ain, float2& ajn) {
+    float t[7];
+    move_trig<VARIANT>(w, t);
+    propose_with<VARIANT>(ai, aj, t, ain, ajn);
 }
 
 // ---------------------------------------------------------------- TMA ring

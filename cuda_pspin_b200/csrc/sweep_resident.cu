@@ -1,34 +1,55 @@
 // sweep_resident.cu -- the plain pair-rotation sweep for samples whose whole
 // set of site lists fits in shared memory next to the amplitudes (sparse
-// samples: ~8 list entries per site), one warp per replica block.
+// samples: ~8 list entries per site).
 //
 // Same moves, RNG streams and Metropolis rule as sweep_kernel.  The lists
 // are copied into shared memory once per launch, so a move reads them
-// without TMA copies or barriers; the 32 lanes evaluate the pair picks of
-// the next 32 moves with one Philox call each; every move runs
-// warp-synchronously (no CTA barrier).  Site m's list is the contiguous
-// range of its chunks (groups or tiles never span chunks; the padding entry
-// of an odd chunk is an empty group).
+// without TMA copies; site m's list is the contiguous range of its chunks
+// (groups or tiles never span chunks; the padding entry of an odd chunk is
+// an empty group).
+//
+// Concurrent commuting moves.  With K warps per replica block, the moves
+// are taken in windows of 32: the lanes of warp 0 draw the window's pair
+// picks (one Philox call each) and mark, for every move, the earlier moves
+// of the window it does not commute with -- move b does not commute with
+// move a when one of b's sites is a site of a or shares a quartet (or a g2
+// term) with one: then b's proposal or fields would read an amplitude that a
+// changes.  The window is cut greedily, in move order, into batches of at
+// most K moves that pairwise commute, and the warps run the moves of a batch
+// at once, warp w the batch's w-th move, each for the block's 32 replicas.
+// Moves that commute give the same result in either order (the same fields,
+// proposals and decisions on the same random words), so a batch equals the
+// same moves run one after another, and the chain is the one-warp chain
+// bit for bit: the running energy adds the moves' dE in move order.  One CTA
+// barrier per batch.  At N=512 with N selected quartets a batch holds ~3.9
+// moves with K=8.
 #include "sweep_common.cuh"
 #include "../../include/pspin.h"
 
 namespace pspin {
 
-// amplitudes [(N+1)][32] float2 ((N+1)*256 bytes), the sample's list entries
-// (16-byte aligned there: tiles are read as int4), site ranges [N] int2,
-// pair picks [32] int2
-inline size_t resident_smem_bytes(int N, int64_t entries) {
-    return (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)entries * sizeof(int2) + (size_t)N * sizeof(int2) +
-           32 * sizeof(int2);
+// Shared memory: amplitudes [(N+1)][32] float2 ((N+1)*256 bytes, so the list
+// entries that follow are 16-byte aligned: tiles are read as int4), the
+// sample's list entries, site ranges [N] int2, pair picks [32] int2,
+// conflict masks [32] u32, batch bounds [34] int, per-batch dE and decisions
+// [2][K][32] (float, int), neighbour masks [N][ceil(N/32)] u32 (K > 1 only).
+inline size_t resident_smem_bytes(int N, int64_t entries, int K) {
+    size_t b = (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)entries * sizeof(int2) + (size_t)N * sizeof(int2) +
+               32 * sizeof(int2) + 32 * sizeof(uint32_t) + 34 * sizeof(int) +
+               (size_t)2 * K * kRepBlock * (sizeof(float) + sizeof(int));
+    if (K > 1) b += (size_t)N * ((N + 31) / 32) * sizeof(uint32_t);
+    return b;
 }
 
 template <int VARIANT>
-__global__ void __launch_bounds__(32) sweep_resident_kernel(const SweepParams P) {
+__global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Unit U = P.units[blockIdx.x];
     const SampleDev S = P.samples[U.sample];
     const int N = S.N, R = S.R;
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int K = (int)(blockDim.x >> 5);
+    const int wpr = (N + 31) >> 5;             // words per neighbour-mask row
     const int* sc = P.site_chunks + S.split_off;
     const int64_t e0 = __ldg(P.chunk_start + __ldg(sc));
     const int64_t e1 = __ldg(P.chunk_start + __ldg(sc + (int64_t)(N - 1) * (kSplit + 1) + kSplit));
@@ -36,19 +57,26 @@ __global__ void __launch_bounds__(32) sweep_resident_kernel(const SweepParams P)
     int2* L = reinterpret_cast<int2*>(sp + (size_t)(N + 1) * kRepBlock);
     int2* rng_site = L + (e1 - e0);
     int2* picks = rng_site + N;
-    for (int m = lane; m < N; m += 32) {
+    uint32_t* cm = reinterpret_cast<uint32_t*>(picks + 32);
+    int* bounds = reinterpret_cast<int*>(cm + 32);             // [0..32] batch starts, [33] batch count
+    float* dEx = reinterpret_cast<float*>(bounds + 34);        // [2][K][32]
+    int* acx = reinterpret_cast<int*>(dEx + 2 * K * kRepBlock);  // [2][K][32]
+    uint32_t* nbm = reinterpret_cast<uint32_t*>(acx + 2 * K * kRepBlock);
+    for (int m = threadIdx.x; m < N; m += blockDim.x) {
         const int64_t b = __ldg(P.chunk_start + __ldg(sc + (int64_t)m * (kSplit + 1)));
         const int64_t e = __ldg(P.chunk_start + __ldg(sc + (int64_t)m * (kSplit + 1) + kSplit));
         rng_site[m] = make_int2((int)(b - e0), (int)(e - e0));
     }
-    for (int64_t t = lane; t < e1 - e0; t += 32) L[t] = P.entries[e0 + t];
-    for (int idx = lane; idx < N * kRepBlock; idx += 32) {
+    for (int64_t t = threadIdx.x; t < e1 - e0; t += blockDim.x) L[t] = P.entries[e0 + t];
+    for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
         const int site = idx >> 5, l = idx & 31;
         float2 v = make_float2(1.f, 0.f);
         if (l < U.rep_count) v = P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l];
         sp[idx] = v;
     }
-    sp[N * kRepBlock + lane] = make_float2(1.f, 0.f);     // virtual site
+    if (threadIdx.x < kRepBlock) sp[N * kRepBlock + threadIdx.x] = make_float2(1.f, 0.f);   // virtual site
+    if (K > 1)
+        for (int t = threadIdx.x; t < N * wpr; t += blockDim.x) nbm[t] = __ldg(P.nbmask + S.nb_off + t);
 
     const bool active = lane < U.rep_count;
     const int64_t gr = S.rep_off + U.rep_begin + lane;
@@ -57,100 +85,155 @@ __global__ void __launch_bounds__(32) sweep_resident_kernel(const SweepParams P)
     long long nacc = 0, nprop = 0;
     uint32_t k0 = 0, k1 = 0;
     if (active) {
-        E = P.energy[gr];
         beta_d = P.beta[gr];
         beta = (float)beta_d;
         const uint64_t key = P.key[gr];
         k0 = (uint32_t)key;
         k1 = (uint32_t)(key >> 32);
+        if (warp == 0) E = P.energy[gr];
     }
     const long long sweep0 = *P.sweep_counter;
     const int steps = N / 2, total = P.nsweeps * steps;
-    __syncwarp();
+    // is `site` a site of move q or a neighbour of one?
+    auto in_reach = [&](int site, int2 q) {
+        return site == q.x || site == q.y || ((nbm[q.x * wpr + (site >> 5)] >> (site & 31)) & 1u) ||
+               ((nbm[q.y * wpr + (site >> 5)] >> (site & 31)) & 1u);
+    };
+    // warp 0's running energy and counters take a batch's moves in move order
+    auto account = [&](int par, int n) {
+        for (int w = 0; w < n; w++) {
+            if (acx[(par * K + w) * kRepBlock + lane]) {
+                E += (double)dEx[(par * K + w) * kRepBlock + lane];
+                nacc++;
+            }
+            nprop++;
+        }
+    };
+    __syncthreads();
 
-    for (int m = 0; m < total; m++) {
-        if ((m & 31) == 0) {                   // pair picks of moves m .. m+31, one per lane
-            const int mm = m + lane;
+    long long batches = 0;
+    int prev = 0;                              // moves in the previous batch
+    for (int m0 = 0; m0 < total; m0 += 32) {
+        const int n = min(32, total - m0);
+        if (warp == 0) {                       // the window's pairs and batches
             int i0 = 0, j0 = 1;
-            if (mm < total)
-                pair_pick(S.pair_key0, S.pair_key1, (uint64_t)(sweep0 + mm / steps), (uint32_t)(mm % steps), N, i0, j0);
+            if (lane < n)
+                pair_pick(S.pair_key0, S.pair_key1, (uint64_t)(sweep0 + (m0 + lane) / steps),
+                          (uint32_t)((m0 + lane) % steps), N, i0, j0);
             picks[lane] = make_int2(i0, j0);
             __syncwarp();
-        }
-        const long long sw = sweep0 + m / steps;
-        const int k = m % steps;
-        const int2 pq = picks[m & 31];
-        const int i0 = pq.x, j0 = pq.y;
-        const U4 w = move_words(k0, k1, (uint64_t)sw, (uint32_t)k);
-        const float2 ai = sp[i0 * kRepBlock + lane], aj = sp[j0 * kRepBlock + lane];
-        float2 ain, ajn;
-        propose<VARIANT>(ai, aj, w, ain, ajn);
-        const float cu = u01f(w.w);
-        sp[j0 * kRepBlock + lane] = ajn;       // h_i is evaluated at the proposed a_j
-        __syncwarp();
-        float hix = 0.f, hiy = 0.f, hjx = 0.f, hjy = 0.f;
-        const int2 ri = rng_site[i0], rj = rng_site[j0];
-        if (S.fc_tiles) {
-            accumulate_tiles(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
-            accumulate_tiles(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
-        } else {
-            accumulate_chunk(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
-            accumulate_chunk(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
-        }
-        const float dix = ain.x - ai.x, diy = ain.y - ai.y;
-        const float djx = ajn.x - aj.x, djy = ajn.y - aj.y;
-        const float dE = -fmaf(dix, hix, -diy * hiy) - fmaf(djx, hjx, -djy * hjy);
-        bool accept;
-        if (beta_d == 0.0) accept = true;
-        else accept = (dE <= 0.f) || (cu < expf(-beta * dE));
-        __syncwarp();
-        if (accept) {
-            sp[i0 * kRepBlock + lane] = ain;
-            E += (double)dE;
-            nacc++;
-        } else {
-            sp[j0 * kRepBlock + lane] = aj;
-        }
-        nprop++;
-        if (P.trace != nullptr && U.sample == P.trace_sample && U.rep_begin + lane == P.trace_rep && active) {
-            const long long idx = (sw - P.trace_sweep0) * steps + k;
-            if (idx >= 0 && idx < P.trace_cap) {
-                pspin_move_record* rec = reinterpret_cast<pspin_move_record*>(P.trace) + idx;
-                rec->i0 = i0; rec->j0 = j0;
-                rec->ai_old[0] = ai.x; rec->ai_old[1] = ai.y;
-                rec->aj_old[0] = aj.x; rec->aj_old[1] = aj.y;
-                rec->ai_new[0] = ain.x; rec->ai_new[1] = ain.y;
-                rec->aj_new[0] = ajn.x; rec->aj_new[1] = ajn.y;
-                rec->dE = dE;
-                rec->accepted = accept ? 1 : 0;
-                rec->log_q_ratio = 0.f;
-                rec->log_u = logf(cu);
+            if (K > 1) {
+                uint32_t mask = 0;
+                for (int j = 0; j < lane && lane < n; j++) {
+                    const int2 q = picks[j];
+                    if (in_reach(i0, q) || in_reach(j0, q)) mask |= 1u << j;
+                }
+                cm[lane] = mask;
+                __syncwarp();
+                if (lane == 0) {
+                    int nb = 0;
+                    for (int s0 = 0; s0 < n;) {
+                        int e = s0 + 1;
+                        uint32_t span = 1u << s0;
+                        while (e < n && e - s0 < K && (cm[e] & span) == 0) {
+                            span |= 1u << e;
+                            e++;
+                        }
+                        bounds[nb++] = s0;
+                        s0 = e;
+                    }
+                    bounds[nb] = n;
+                    bounds[33] = nb;
+                }
+            } else if (lane == 0) {
+                for (int b = 0; b <= n; b++) bounds[b] = b;
+                bounds[33] = n;
             }
         }
-        __syncwarp();
+        __syncthreads();
+        const int nb = bounds[33];
+        for (int b = 0; b < nb; b++) {
+            const int bs = bounds[b], be = bounds[b + 1];
+            const int par = (int)(batches & 1);
+            if (warp == 0 && batches > 0) account(par ^ 1, prev);
+            if (warp < be - bs) {
+                const int m = m0 + bs + warp;
+                const long long sw = sweep0 + m / steps;
+                const int k = m % steps;
+                const int2 pq = picks[bs + warp];
+                const int i0 = pq.x, j0 = pq.y;
+                const U4 w = move_words(k0, k1, (uint64_t)sw, (uint32_t)k);
+                const float2 ai = sp[i0 * kRepBlock + lane], aj = sp[j0 * kRepBlock + lane];
+                float2 ain, ajn;
+                propose<VARIANT>(ai, aj, w, ain, ajn);
+                const float cu = u01f(w.w);
+                sp[j0 * kRepBlock + lane] = ajn;       // h_i is evaluated at the proposed a_j
+                __syncwarp();
+                float hix = 0.f, hiy = 0.f, hjx = 0.f, hjy = 0.f;
+                const int2 ri = rng_site[i0], rj = rng_site[j0];
+                if (S.fc_tiles) {
+                    accumulate_tiles(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
+                    accumulate_tiles(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
+                } else {
+                    accumulate_chunk(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
+                    accumulate_chunk(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
+                }
+                const float dix = ain.x - ai.x, diy = ain.y - ai.y;
+                const float djx = ajn.x - aj.x, djy = ajn.y - aj.y;
+                const float dE = -fmaf(dix, hix, -diy * hiy) - fmaf(djx, hjx, -djy * hjy);
+                bool accept;
+                if (beta_d == 0.0) accept = true;
+                else accept = (dE <= 0.f) || (cu < expf(-beta * dE));
+                __syncwarp();
+                if (accept) sp[i0 * kRepBlock + lane] = ain;
+                else sp[j0 * kRepBlock + lane] = aj;
+                dEx[(par * K + warp) * kRepBlock + lane] = dE;
+                acx[(par * K + warp) * kRepBlock + lane] = accept ? 1 : 0;
+                if (P.trace != nullptr && U.sample == P.trace_sample && U.rep_begin + lane == P.trace_rep && active) {
+                    const long long idx = (sw - P.trace_sweep0) * steps + k;
+                    if (idx >= 0 && idx < P.trace_cap) {
+                        pspin_move_record* rec = reinterpret_cast<pspin_move_record*>(P.trace) + idx;
+                        rec->i0 = i0; rec->j0 = j0;
+                        rec->ai_old[0] = ai.x; rec->ai_old[1] = ai.y;
+                        rec->aj_old[0] = aj.x; rec->aj_old[1] = aj.y;
+                        rec->ai_new[0] = ain.x; rec->ai_new[1] = ain.y;
+                        rec->aj_new[0] = ajn.x; rec->aj_new[1] = ajn.y;
+                        rec->dE = dE;
+                        rec->accepted = accept ? 1 : 0;
+                        rec->log_q_ratio = 0.f;
+                        rec->log_u = logf(cu);
+                    }
+                }
+            }
+            __syncthreads();
+            prev = be - bs;
+            batches++;
+        }
     }
-    for (int idx = lane; idx < N * kRepBlock; idx += 32) {
+    if (warp == 0 && batches > 0) account((int)((batches - 1) & 1), prev);
+    for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
         const int site = idx >> 5, l = idx & 31;
         if (l < U.rep_count) P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l] = sp[idx];
     }
-    if (active) {
+    if (warp == 0 && active) {
         P.energy[gr] = E;
         P.accepted[gr] += nacc;
         P.proposed[gr] += nprop;
     }
 }
 
-size_t resident_smem_bytes_host(int N, int64_t entries) { return resident_smem_bytes(N, entries); }
+size_t resident_smem_bytes_host(int N, int64_t entries, int warps) { return resident_smem_bytes(N, entries, warps); }
 
 cudaError_t launch_sweep_resident(const SweepParams& p, int n_units, int variant, int max_N, int64_t max_entries,
                                   cudaStream_t st) {
     if (n_units <= 0) return cudaSuccess;
-    const size_t smem = resident_smem_bytes(max_N, max_entries);
+    if (p.warps < 1 || p.warps > 8) return cudaErrorInvalidValue;
+    const size_t smem = resident_smem_bytes(max_N, max_entries, p.warps);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     auto kern = variant == 0 ? sweep_resident_kernel<0> : sweep_resident_kernel<1>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<n_units, 32, smem, st>>>(p);
+    kern<<<n_units, 32 * p.warps, smem, st>>>(p);
     return cudaGetLastError();
 }
 

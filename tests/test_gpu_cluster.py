@@ -70,3 +70,30 @@ def test_cluster_option_checks(ps):
             ps.Engine(c, ps.PSPIN_DENSE, ps.make_options(cluster_size=bad))
     with pytest.raises(ps.PspinError):
         ps.Engine(c, ps.PSPIN_DENSE, ps.make_options(cluster_size=16, warps_per_unit=4))
+
+
+@pytest.mark.parametrize("variant,kw", [
+    (1, dict(N=512, nrep=64, fmc_mode=1, seed=42, gamma=1.0)),     # sparse cube, comb: batches of ~4 moves
+    (1, dict(N=64, nrep=40, fmc_mode=2, seed=8, gamma=0.05)),      # sparse, uniform FMC (H2 active: batches of 1)
+    (1, dict(N=96, nrep=33, fmc_mode=0, seed=3)),                  # sparse, fully connected selection
+    (0, dict(N=12, nrep=33, fmc_mode=2, seed=7)),                  # dense groups (every move conflicts)
+])
+def test_resident_batched_moves_equal_one_warp(ps, variant, kw):
+    """The list-resident kernel with K warps runs batches of consecutive
+    moves that commute concurrently; the chain must equal the one-warp
+    chain bit for bit (amplitudes, running energies, counters)."""
+    c = ps.default_config(**kw)
+    if c.fmc_mode == 2 and c.gamma <= 0.0:
+        c.gamma = 1.0 / (2.0 * (c.N - 1))
+    out = []
+    for K in (1, 2, 4, 8):
+        with ps.Engine(c, variant, ps.make_options(resync_every=-1, cluster_size=-1, warps_per_unit=K)) as eng:
+            eng.fill_betas(1.0 / 0.4)
+            eng.sweep(6)
+            E, acc, prop = eng.get_results()
+            out.append((eng.get_spins()[0], E, acc, prop))
+    for K, o in zip((2, 4, 8), out[1:]):
+        np.testing.assert_array_equal(o[0], out[0][0], err_msg=f"amplitudes, K={K}")
+        for i in (1, 2, 3):
+            np.testing.assert_array_equal(o[i], out[0][i], err_msg=f"K={K}")
+    assert np.all(out[0][2] > 0)
