@@ -124,6 +124,18 @@ def load_library() -> ctypes.CDLL:
         "pspin_fmc_survivors_static": (ctypes.c_int, [ctypes.c_int, vp, ctypes.c_double, vp, vp]),
         "pspin_local_fields": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp, vp]),
         "pspin_sweep_work": (ctypes.c_int, [vp, vp, vp]),
+        "pspin_device_arrays": (ctypes.c_int, [vp, vp, vp, vp, vp]),
+        "pspin_deeper_counts": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_double, vp, ctypes.c_int,
+                                               vp, vp, vp, vp, vp]),
+        "pspin_multi_overlap": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp,
+                                               ctypes.c_int, vp]),
+        "pspin_std_shuffle": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, vp]),
+        "pspin_reservoir_sample": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, vp, ctypes.c_int,
+                                                  ctypes.c_uint32, vp, vp]),
+        "pspin_fy_downsample": (ctypes.c_int, [ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_uint32,
+                                               vp, vp]),
+        "pspin_tau_e": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, vp, vp]),
         "pspin_set_proposal": (ctypes.c_int, [vp, ctypes.c_int]),
         "pspin_observe_init": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
         "pspin_autotune": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp]),

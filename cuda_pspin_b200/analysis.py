@@ -11,6 +11,12 @@ exactly as the reference bins:
     experimental IFO of the time-averaged spectra, once per pair
     (`pspin_ifo_counts`; analysis_pt.cpp:1498-1663 -> ifo_overlap.dat,
     :1679-1850 -> exp_ifo_overlap.dat).
+With --deeper, as analysis_pt --deeper does: P(|a|^2) and the inverse
+participation ratios, the phase overlap and, for runs with quartets.txt,
+the link overlap and the q-q_link scatter (`pspin_deeper_counts`,
+analysis_pt.cpp:1871-2290), and the multi-overlap scatter files
+(`pspin_multi_overlap`, :3468-3643).  Always: the energy decorrelation time
+tau_E (decorrelation_time.dat, :2694-2790; `pspin_tau_e` on the host).
 Each sample's histogram is normalised to a density and the files hold the
 sample mean and jackknife error in the reference's format; from the same
 histograms, as analysis_pt does for each distribution (tags parisi, ifo,
@@ -21,11 +27,12 @@ jackknife errors, analysis_pt.cpp:61-126), {tag}_glass_observables.dat (chi
 IEEE doubles, so the printed numbers are the reference's (a single sample
 gives its -nan jackknife errors):
 
-    python -m cuda_pspin_b200.analysis -N 12 -NT 4 -nrep 2 [-nbins 100] [--data data] [--out analysis_gpu]
+    python -m cuda_pspin_b200.analysis -N 12 -NT 4 -nrep 2 [-nbins 100] [--deeper] [--data data] [--out analysis_gpu]
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import math
 import os
 import re
@@ -295,6 +302,266 @@ def write_glass_observables(outdir: str, tag: str, hists: np.ndarray, temps, N: 
             out.write("%.8f" % temps[ti] + "".join("\t" + _e(x2[s][ti]) for s in range(S)) + "\n")
 
 
+def read_quartets(d: str) -> np.ndarray:
+    """quartets.txt of a sparse run as [M, 5] int32 (i, j, k, l, ch); empty
+    when the file is absent (analysis_pt.cpp:314-330)."""
+    path = os.path.join(d, "quartets.txt")
+    rows = []
+    if os.path.isfile(path):
+        with open(path) as f:
+            for line in f:
+                if line.startswith("#") or line.startswith("\n"):
+                    continue
+                tok = line.split()
+                if len(tok) >= 7:
+                    try:
+                        rows.append([int(tok[1]), int(tok[2]), int(tok[3]), int(tok[4]), int(tok[5])])
+                        float(tok[6])
+                    except ValueError:
+                        continue
+    return np.array(rows, np.int32).reshape(-1, 5)
+
+
+def energy_rows(d: str, NT: int, nrep: int) -> list[np.ndarray]:
+    """energy_accept.txt's E/N columns per temperature index, rows in file
+    order ([M_t, nrep] each; analysis_pt.cpp:501-565)."""
+    out = [[] for _ in range(NT)]
+    with open(os.path.join(d, "energy_accept.txt")) as f:
+        for line in f:
+            if line.startswith("#") or line.startswith("\n"):
+                continue
+            tok = line.split()
+            if len(tok) < 3 + 2 * nrep:
+                continue
+            t = int(tok[1])
+            if 0 <= t < NT:
+                out[t].append([float(tok[3 + 2 * r]) for r in range(nrep)])
+    return [np.array(r, np.float64).reshape(-1, nrep) for r in out]
+
+
+def tau_e(rows: np.ndarray) -> float:
+    """The reference's tau_E of one temperature (pspin_tau_e)."""
+    r = np.ascontiguousarray(rows, np.float64)
+    t = ctypes.c_double()
+    if load_library().pspin_tau_e(int(r.shape[0]), int(r.shape[1]), _ptr(r), ctypes.byref(t)) != 0:
+        raise ValueError("pspin_tau_e: bad arguments")
+    return t.value
+
+
+def write_tau_e(outdir: str, runs, NT: int, nrep: int, temps) -> str:
+    """decorrelation_time.dat: tau_E per temperature, sample mean and
+    jackknife error (analysis_pt.cpp:2755-2788)."""
+    S = len(runs)
+    tau = [[0.0] * NT for _ in range(S)]
+    for s, (_, d) in enumerate(runs):
+        rows = energy_rows(d, NT, nrep)
+        for ti in range(NT):
+            tau[s][ti] = tau_e(rows[ti])
+    path = os.path.join(outdir, "decorrelation_time.dat")
+    with open(path, "w") as f:
+        f.write("# Energy decorrelation time tau_E (in save_freq units)\n")
+        f.write("# T\ttau_E\ttau_E_err\n")
+        for ti in range(NT):
+            vals = [tau[s][ti] for s in range(S)]
+            fm = 0.0
+            for v in vals:
+                fm += v
+            fm = _div(fm, S)
+            jk = 0.0
+            for j in range(S):
+                lv = 0.0
+                for s in range(S):
+                    if s != j:
+                        lv += vals[s]
+                lv = _div(lv, S - 1)
+                jk += (lv - fm) * (lv - fm)
+            jk = math.sqrt((S - 1.0) / S * jk) if S > 0 else float("nan")
+            f.write("%.8f\t%s\t%s\n" % (temps[ti], _e(fm), _e(jk)))
+    return path
+
+
+NBINS_A2, A2_MAX = 100, 10.0
+MARGINAL_HEADER = ["# Marginal distribution P(|a_k|^2 = I_k)", "# Columns: I_center  P(I)  Error_jk  Temperature"]
+PHASE_HEADER = ["# Phase overlap distribution P(q_phi)", "# q_phi = (1/N_eff) sum_k cos(theta_k^a - theta_k^b)",
+                "# Columns: q_phi_center  P(q_phi)  Error_jk  Temperature"]
+LINK_HEADER = ["# Link overlap distribution P(q_link)",
+               "# q_link = (1/M) sum_q t_q(a)*t_q(b),  t_q = Re[prod with channel]",
+               "# Columns: q_link_center  P(q_link)  Error_jk  Temperature"]
+
+
+def deeper_sample(cfg: np.ndarray, nbins: int, quarts: np.ndarray):
+    """One sample's deeper-block results (analysis_pt.cpp:1871-2045):
+    marginal, phase and link densities [NT, bins], Y2 and Y4 per temperature
+    and the (q, q_link) scatter points per temperature, normalised in the
+    reference's order."""
+    nsnap, NT, nrep, N, _ = cfg.shape
+    npairs = nrep * (nrep - 1) // 2
+    M = int(quarts.shape[0])
+    marg = np.zeros((NT, NBINS_A2), np.int64)
+    phase = np.zeros((NT, nbins), np.int64)
+    link = np.zeros((NT, nbins), np.int64)
+    y = np.zeros((nsnap, NT, nrep, 3))
+    sc = np.zeros((NT, nsnap, npairs, 2))
+    c = np.ascontiguousarray(cfg, np.float64)
+    q = np.ascontiguousarray(quarts, np.int32) if M else np.zeros((1, 5), np.int32)
+    _check(load_library().pspin_deeper_counts(N, NT, nrep, nsnap, _ptr(c), nbins, NBINS_A2, A2_MAX, _ptr(q), M,
+                                              _ptr(marg), _ptr(y), _ptr(phase), _ptr(link), _ptr(sc)))
+    da2 = A2_MAX / NBINS_A2
+    dq = 2.0 / nbins
+    md, pd, ld = marg.astype(np.float64), phase.astype(np.float64), link.astype(np.float64)
+    y2, y4, scat = [0.0] * NT, [0.0] * NT, []
+    for t in range(NT):
+        n_ipr, a2, a4 = 0, 0.0, 0.0
+        for sn in range(nsnap):
+            for r in range(nrep):
+                if y[sn, t, r, 2] != 0.0:
+                    a2 += float(y[sn, t, r, 0])
+                    a4 += float(y[sn, t, r, 1])
+                    n_ipr += 1
+        if n_ipr * N > 0:
+            md[t] = md[t] / (float(n_ipr * N) * da2)
+        if n_ipr > 0:
+            a2 /= n_ipr
+            a4 /= n_ipr
+        y2[t], y4[t] = a2, a4
+        n_ph = nsnap * npairs
+        if n_ph > 0:
+            pd[t] = pd[t] / (n_ph * dq)
+            if M:
+                ld[t] = ld[t] / (n_ph * dq)
+        scat.append(sc[t].reshape(-1, 2) if M else np.zeros((0, 2)))
+    return md, pd, ld, np.array(y2), np.array(y4), scat
+
+
+def _write_ipr(outdir: str, y2: np.ndarray, y4: np.ndarray, temps) -> list[str]:
+    S, NT = y2.shape
+    ff = math.sqrt((S - 1.0) / S)
+    p1, p2 = os.path.join(outdir, "ipr.dat"), os.path.join(outdir, "ipr_sample.dat")
+    with open(p1, "w") as f:
+        f.write("# Inverse Participation Ratios\n")
+        f.write("# Y2 = sum I_k^2 / (sum I_k)^2,  Y4 = sum I_k^4 / (sum I_k)^4\n")
+        f.write("# 1/Y2 = effective number of participating modes\n")
+        f.write("# Columns: T  Y2  Y2_err  Y4  Y4_err\n")
+        for ti in range(NT):
+            y2f = y4f = 0.0
+            for s in range(S):
+                y2f += float(y2[s, ti])
+                y4f += float(y4[s, ti])
+            y2f = _div(y2f, S)
+            y4f = _div(y4f, S)
+            j2 = j4 = 0.0
+            for j in range(S):
+                l2 = l4 = 0.0
+                for s in range(S):
+                    if s != j:
+                        l2 += float(y2[s, ti])
+                        l4 += float(y4[s, ti])
+                l2 = _div(l2, S - 1)
+                l4 = _div(l4, S - 1)
+                j2 += (l2 - y2f) * (l2 - y2f)
+                j4 += (l4 - y4f) * (l4 - y4f)
+            f.write("%.8f\t%s\t%s\t%s\t%s\n" % (temps[ti], _e(y2f), _e(ff * math.sqrt(j2)), _e(y4f),
+                                                   _e(ff * math.sqrt(j4))))
+    with open(p2, "w") as f:
+        f.write("# Per-sample Y2 values\n")
+        f.write("# Columns: T  sample_0  sample_1  ... sample_{n-1}\n")
+        for ti in range(NT):
+            f.write("%.8f" % temps[ti] + "".join("\t" + _e(float(y2[s, ti])) for s in range(S)) + "\n")
+    return [p1, p2]
+
+
+def write_deeper(outdir: str, runs, N: int, NT: int, nrep: int, nbins: int, temps) -> list[str]:
+    """Every file of analysis_pt's deeper overlap block (P(|a|^2), IPR, phase
+    and link overlaps with their moments and glass observables, the
+    q-q_link scatter) and the multi-overlap scatter files."""
+    os.makedirs(outdir, exist_ok=True)
+    marg, phase, link, y2, y4, scat, has_q = [], [], [], [], [], [], False
+    multi = [[] for _ in range(NT)]
+    lib = load_library()
+    npairs = nrep * (nrep - 1) // 2
+    for s, (_, d) in enumerate(runs):
+        cfg = read_configs(d, N, NT, nrep)
+        quarts = read_quartets(d)
+        has_q = has_q or quarts.shape[0] > 0
+        m, p, l, a, b, sc = deeper_sample(cfg, nbins, quarts)
+        marg.append(m); phase.append(p); link.append(l); y2.append(a); y4.append(b); scat.append(sc)
+        # multi-overlap: snapshots in sweep order, shuffled and cut to 512 when more
+        nsnap = cfg.shape[0]
+        nit = min(nsnap, 512)
+        snaps = np.zeros((NT, max(nit, 1)), np.int32)
+        for ti in range(NT):
+            idx = np.arange(nsnap, dtype=np.int32)
+            if nsnap > 512:
+                _check_rc(lib.pspin_std_shuffle(nsnap, (42 + s * NT + ti) & 0xFFFFFFFF, _ptr(idx)))
+            snaps[ti, :nit] = idx[:nit]
+        if nit > 0:
+            out = np.zeros((NT, npairs, nit, 3))
+            c = np.ascontiguousarray(cfg, np.float64)
+            _check(lib.pspin_multi_overlap(N, NT, nrep, nsnap, _ptr(c), _ptr(snaps), nit, _ptr(out)))
+            for ti in range(NT):
+                multi[ti].append(out[ti].reshape(-1, 3))
+    paths = []
+    da2 = A2_MAX / NBINS_A2
+    path = os.path.join(outdir, "marginal_a2.dat")
+    write_parisi_overlap(path, np.stack(marg), temps, N, NT, nrep, NBINS_A2, 0.0, A2_MAX, header=MARGINAL_HEADER)
+    paths.append(path)
+    paths += _write_ipr(outdir, np.stack(y2), np.stack(y4), temps)
+    for tag, hists, header, mheader in (("phase", phase, PHASE_HEADER, "Moments of P(q_phi)"),
+                                        ("link", link, LINK_HEADER, "Moments of P(q_link)")):
+        if tag == "link" and not has_q:
+            continue
+        h = np.stack(hists)
+        path = os.path.join(outdir, "%s_overlap.dat" % tag)
+        write_parisi_overlap(path, h, temps, N, NT, nrep, nbins, header=header)
+        write_moments(os.path.join(outdir, "%s_moments.dat" % tag), mheader, h, temps, nbins)
+        write_glass_observables(outdir, tag, h, temps, N, nbins)
+        paths += [path, os.path.join(outdir, "%s_moments.dat" % tag),
+                  os.path.join(outdir, "%s_glass_observables.dat" % tag),
+                  os.path.join(outdir, "%s_sample_x2.dat" % tag)]
+    if has_q:
+        counts = np.array([sum(sc[ti].shape[0] for sc in scat) for ti in range(NT)], np.int64)
+        pts = np.ascontiguousarray(np.concatenate([np.concatenate([sc[ti] for sc in scat]) for ti in range(NT)]),
+                                   np.float64).reshape(-1, 2)
+        kept = np.zeros_like(pts)
+        kc = np.zeros(NT, np.int64)
+        _check_rc(lib.pspin_fy_downsample(NT, _ptr(counts), 2, _ptr(pts), 2000, 42, _ptr(kept), _ptr(kc)))
+        path = os.path.join(outdir, "scatter_q_qlink.dat")
+        with open(path, "w") as f:
+            f.write("# Scatter: Parisi overlap q vs Link overlap q_link\n")
+            f.write("# Columns: q_parisi  q_link  Temperature\n")
+            f.write("# (downsampled to max %d points per temperature)\n" % 2000)
+            off = 0
+            for ti in range(NT):
+                f.write("\n")
+                for p_ in kept[off:off + kc[ti]]:
+                    f.write("%s\t%s\t%.8f\n" % (_e(float(p_[0])), _e(float(p_[1])), temps[ti]))
+                off += kc[ti]
+        paths.append(path)
+    for ti in range(NT):
+        if not multi[ti]:
+            continue
+        pts = np.ascontiguousarray(np.concatenate(multi[ti]), np.float64)
+        kept = np.zeros((5000, 3))
+        nk = ctypes.c_longlong()
+        _check_rc(lib.pspin_reservoir_sample(pts.shape[0], 3, _ptr(pts), 5000, (42 + ti) & 0xFFFFFFFF, _ptr(kept),
+                                             ctypes.byref(nk)))
+        if nk.value == 0:
+            continue
+        path = os.path.join(outdir, "multi_overlap_T%.4f.dat" % temps[ti])
+        with open(path, "w") as f:
+            f.write("# Multi-overlap scatter at T=%.6f\n" % temps[ti])
+            f.write("# q_parisi\tq_phase\tIFO\n")
+            for p_ in kept[:nk.value]:
+                f.write("%s\t%s\t%s\n" % (_e(float(p_[0])), _e(float(p_[1])), _e(float(p_[2]))))
+        paths.append(path)
+    return paths
+
+
+def _check_rc(rc: int) -> None:
+    if rc != 0:
+        raise ValueError("bad arguments to a sampling helper")
+
+
 # the three distributions: file stem / tag, moments header, distribution header
 DISTRIBUTIONS = (("parisi", "Moments of P(q)", PARISI_HEADER),
                  ("ifo", "Moments of P(C) [IFO]", IFO_HEADER),
@@ -325,6 +592,7 @@ def main(argv=None) -> int:
     ap.add_argument("-nbins", type=int, default=100)
     ap.add_argument("--data", default="data")
     ap.add_argument("--out", default="analysis_gpu")
+    ap.add_argument("--deeper", action="store_true", help="also the deeper block and the multi-overlap scatter")
     a = ap.parse_args(argv)
     runs = find_runs(a.data, a.N, a.NT, a.nrep)
     if not runs:
@@ -340,6 +608,9 @@ def main(argv=None) -> int:
     temps = temperatures(runs[0][1], a.NT)
     paths = write_all(a.out, {"parisi": np.stack(hists), "ifo": np.stack(ifo), "exp_ifo": np.stack(exp_ifo)},
                       temps, a.N, a.NT, a.nrep, a.nbins)
+    paths.append(write_tau_e(a.out, runs, a.NT, a.nrep, temps))
+    if a.deeper:
+        paths += write_deeper(a.out, runs, a.N, a.NT, a.nrep, a.nbins, temps)
     for path in paths:
         print("%d samples, written %s" % (len(runs), path))
     return 0

@@ -1695,6 +1695,35 @@ extern "C" int pspin_ifo_counts(int N, int NT, int nrep, int nsnap, const double
     return PSPIN_OK;
 }
 
+extern "C" int pspin_deeper_counts_impl(int N, int NT, int nrep, int nsnap, const double* configs, int nbins,
+                                        int nbins_a2, double da2, const int32_t* quartets, int M, long long* marg,
+                                        double* y, long long* phase, long long* link, double* scatter,
+                                        const char** err);
+extern "C" int pspin_deeper_counts(int N, int NT, int nrep, int nsnap, const double* configs, int nbins, int nbins_a2,
+                                   double a2_max, const int32_t* quartets, int M, int64_t* marg, double* ipr_terms,
+                                   int64_t* phase, int64_t* link, double* scatter) {
+    const char* err = nullptr;
+    const int rc = pspin_deeper_counts_impl(N, NT, nrep, nsnap, configs, nbins, nbins_a2,
+                                            nbins_a2 > 0 ? a2_max / nbins_a2 : 0.0, quartets, M,
+                                            reinterpret_cast<long long*>(marg), ipr_terms,
+                                            reinterpret_cast<long long*>(phase), reinterpret_cast<long long*>(link),
+                                            scatter, &err);
+    if (rc == 1) return fail(PSPIN_ERR_ARG, "%s", err);
+    if (rc) return fail(PSPIN_ERR_CUDA, "pspin_deeper_counts: %s", err);
+    return PSPIN_OK;
+}
+
+extern "C" int pspin_multi_overlap_impl(int N, int NT, int nrep, int nsnap, const double* configs,
+                                        const int32_t* snaps, int nit, double* out, const char** err);
+extern "C" int pspin_multi_overlap(int N, int NT, int nrep, int nsnap, const double* configs, const int32_t* snaps,
+                                   int nit, double* out) {
+    const char* err = nullptr;
+    const int rc = pspin_multi_overlap_impl(N, NT, nrep, nsnap, configs, snaps, nit, out, &err);
+    if (rc == 1) return fail(PSPIN_ERR_ARG, "%s", err);
+    if (rc) return fail(PSPIN_ERR_CUDA, "pspin_multi_overlap: %s", err);
+    return PSPIN_OK;
+}
+
 extern "C" int pspin_exchange_host(int n_samples, int NT, int nrep, const double* beta_sched, const double* energy,
                                    const int64_t* rep_off, int32_t* perm, uint64_t* drand_state, int64_t* ex_acc,
                                    int64_t* ex_prop, double* betas) {

@@ -222,6 +222,49 @@ int  pspin_overlap_counts(int N, int NT, int nrep, int nsnap, const double* conf
  * either pair of outputs may be NULL.  Binned as the reference bins. */
 int  pspin_ifo_counts(int N, int NT, int nrep, int nsnap, const double* configs, int nbins, double cmin,
                       double cmax, int64_t* ifo_counts, int64_t* ifo_n, int64_t* exp_counts, int64_t* exp_n);
+/* The deeper analysis of one sample's saved configurations on the GPU
+ * (analysis_pt.cpp:1871-2045, run there with --deeper), same configs
+ * layout, FP64 in the reference's operation order:
+ *   marg [NT][nbins_a2]  counts of I_k = |a_k|^2 in bins of a2_max/nbins_a2
+ *                        (kept when inside [0, nbins_a2)), over every
+ *                        snapshot, replica and site;
+ *   ipr_terms [nsnap][NT][nrep][3]  sum I^2/(sum I)^2, sum I^4/(sum I)^4 and
+ *                        1 per configuration ((0, 0, 0) when sum I = 0);
+ *   phase, link [NT][nbins]  counts of the phase overlap q_phi (mean of
+ *                        cos(theta_a - theta_b) over sites where both
+ *                        |.|^2 > 1e-24) and of the link overlap
+ *                        q_link = sum_q t_q(a) t_q(b) / M over the M
+ *                        quartets [M][5] (i, j, k, l, ch; M = 0: none) per
+ *                        snapshot and pair a < b, bins of 2/nbins on [-1, 1];
+ *   scatter [NT][nsnap][pairs][2]  (q, q_link) per snapshot and pair. */
+int  pspin_deeper_counts(int N, int NT, int nrep, int nsnap, const double* configs, int nbins, int nbins_a2,
+                         double a2_max, const int32_t* quartets, int M, int64_t* marg, double* ipr_terms,
+                         int64_t* phase, int64_t* link, double* scatter);
+/* Multi-overlap values of one sample on the GPU (analysis_pt.cpp:3468-3643):
+ * on the snapshots snaps[t][0..nit) of each temperature, out
+ * [NT][pairs][nit][3] = (q / sqrt(sum I_a sum I_b), phase overlap over sites
+ * with both I > 1e-20, IFO about the mean intensity over those snapshots). */
+int  pspin_multi_overlap(int N, int NT, int nrep, int nsnap, const double* configs, const int32_t* snaps,
+                         int nit, double* out);
+/* The reference's host sampling with the same C++ standard-library engine
+ * and distributions, so sampled points and their order are the reference's:
+ * idx <- 0..n-1 permuted by std::shuffle with std::mt19937(seed)
+ * (analysis_pt.cpp:3504-3507); a reservoir of max_pts points from a stream
+ * (std::uniform_int_distribution<int>(0, seen-1), :3609-3619); and per
+ * block, when it holds more than max_pts points, a partial Fisher-Yates
+ * shuffle with one engine shared by the blocks in order (:2262-2269).
+ * Host only; return 0, or 1 on bad arguments. */
+int  pspin_std_shuffle(int n, uint32_t seed, int32_t* idx);
+int  pspin_reservoir_sample(long long n, int dim, const double* pts, int max_pts, uint32_t seed, double* out,
+                            long long* n_out);
+int  pspin_fy_downsample(int nblocks, const long long* counts, int dim, const double* pts, int max_pts,
+                         uint32_t seed, double* out, long long* out_counts);
+/* The reference's energy decorrelation time tau_E of one temperature
+ * (analysis_pt.cpp:2703-2752): energy [M][nrep] the saved E/N rows in order;
+ * the second half, replica-averaged, and the lag where its autocorrelation
+ * first falls below 1/e, linearly interpolated (in save_freq units).  Host
+ * only; 0, or 1 on bad arguments. */
+int  pspin_tau_e(int M, int nrep, const double* energy, double* tau);
 /* NT, replicas per temperature and exchange period set by pspin_pt_init (0s before). */
 int  pspin_pt_shape(pspin_state* s, int* NT, int* nrep_per_temp, int* pt_freq);
 /* Block-shape autotuner (no reference counterpart): times `sweeps` sweeps

@@ -202,3 +202,52 @@ def test_overlap_files_match_analysis_pt(tmp_path, S):
         assert open(path).read() == open(ref).read(), os.path.basename(path)
     if S == 1:
         assert "-nan" in open(paths[1]).read()
+
+
+@pytest.mark.skipif(not os.path.exists(REF_ANALYSIS), reason="reference analysis_pt not built")
+def test_decorrelation_time_matches_analysis_pt(tmp_path):
+    """tau_E (pspin_tau_e on the host, analysis.write_tau_e) against the
+    reference analysis_pt's decorrelation_time.dat, byte for byte, on
+    synthetic runs whose energy series are AR(1) processes of different
+    correlation per temperature (crossings of 1/e with and without
+    interpolation, a series that never crosses, a constant one)."""
+    N, NT, nrep, nsnap = 6, 4, 3, 2
+    rng = np.random.default_rng(11)
+    M = 80
+    for s in range(3):
+        d = tmp_path / "data" / f"PT_N{N}_a0.5_Rinf_a00.5_NT{NT}_NR{nrep}_S{s}"
+        _fake_run(str(d), N, NT, nrep, nsnap, rng, s)
+        series = np.zeros((NT, M, nrep))
+        for t, phi in enumerate((0.2, 0.8, 0.995, None)):
+            if phi is None:
+                series[t] = -1.25
+                continue
+            x = rng.normal(size=nrep)
+            for i in range(M):
+                x = phi * x + rng.normal(size=nrep)
+                series[t, i] = -1.0 + 0.01 * x
+        with open(d / "energy_accept.txt", "w") as f:
+            f.write("# sweep\tTidx\tT" + "".join(f"\tE{r}/N\tacc{r}" for r in range(nrep)) + "\n")
+            for i in range(M):
+                for t in range(NT):
+                    f.write("%d\t%d\t%.8f" % (10 * (i + 1), t, 1.5 - 0.25 * t) +
+                            "".join("\t%.8f\t0.50000" % series[t, i, r] for r in range(nrep)) + "\n")
+        with open(d / "exchanges.txt", "w") as f:
+            f.write("# sweep\tTidx\tT_high\tT_low\tn_acc\tn_prop\trate\n")
+            for i in range(M):
+                for t in range(NT - 1):
+                    f.write("%d\t%d\t%.8f\t%.8f\t1\t2\t0.50000\n" % (10 * (i + 1), t, 1.5 - 0.25 * t,
+                                                                   1.25 - 0.25 * t))
+    p = subprocess.run([REF_ANALYSIS, "-N", str(N), "-NT", str(NT), "-nrep", str(nrep)],
+                       cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr[-1000:]
+    runs = A.find_runs(str(tmp_path / "data"), N, NT, nrep)
+    temps = A.temperatures(runs[0][1], NT)
+    os.makedirs(tmp_path / "ours")
+    path = A.write_tau_e(str(tmp_path / "ours"), runs, NT, nrep, temps)
+    refdir = [r for r, _, fs in os.walk(tmp_path / "analysis") if "decorrelation_time.dat" in fs]
+    assert len(refdir) == 1
+    ours = open(path).read()
+    assert ours == open(os.path.join(refdir[0], "decorrelation_time.dat")).read()
+    vals = [float(l.split()[1]) for l in ours.splitlines() if not l.startswith("#")]
+    assert vals[0] > 0 and vals[2] > vals[1] > vals[0] and vals[3] == 0.0

@@ -245,3 +245,42 @@ def test_sa_statistics_match_reference(tmp_path):
     print("reference E/N per T:", np.round(obs_r[:, 0].mean(axis=0), 4).tolist())
     assert np.all(np.abs(z) < 3.5), z
     assert np.mean(np.abs(z) < 2.0) >= 0.8, z
+
+
+@pytest.mark.parametrize("variant", ["dense", "sparse"])
+def test_gpu_deeper_analysis_matches_analysis_pt(tmp_path, variant):
+    """The deeper block on the GPU (pspin_deeper_counts, pspin_multi_overlap,
+    the host sampling helpers and cuda_pspin_b200.analysis --deeper) against
+    analysis_pt --deeper on the same runs: marginal_a2.dat, ipr.dat,
+    ipr_sample.dat, the phase overlap with its moments, glass observables and
+    per-sample <x^2>, for the sparse runs (quartets.txt) the link overlap
+    files and the downsampled q-q_link scatter, the multi-overlap scatter
+    file of every temperature, and decorrelation_time.dat -- byte for byte."""
+    sparse = variant == "sparse"
+    N = "16" if sparse else "12"
+    flags = ["-N", N, "-Tmax", "1.6", "-Tmin", "0.3", "-NT", "4", "-log_temp", "-nrep", "3", "-iter", "1024",
+             "-pt_freq", "1", "-save_freq", "8", "-seed", "21", "-label", "0", "-batch", "4"]
+    if sparse:
+        flags += ["-fmc", "1", "-gamma", "1"]
+    run([os.path.join(BIN, "pspin_pt_sparse" if sparse else "pspin_pt"), *flags], tmp_path)
+    run([os.path.join(REF, "analysis_pt"), "-N", N, "-NT", "4", "-nrep", "3", "--log-temp", "--deeper"], tmp_path)
+    p = subprocess.run([sys.executable, "-m", "cuda_pspin_b200.analysis", "-N", N, "-NT", "4", "-nrep", "3",
+                        "--deeper", "--out", str(tmp_path / "gpu")], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=600, env={**os.environ, "PYTHONPATH": ROOT})
+    assert p.returncode == 0, p.stderr[-2000:]
+    refdir = [r for r, _, fs in os.walk(tmp_path / "analysis") if "phase_overlap.dat" in fs]
+    assert len(refdir) == 1
+    names = ["marginal_a2.dat", "ipr.dat", "ipr_sample.dat", "decorrelation_time.dat"]
+    tags = ["phase", "link"] if sparse else ["phase"]
+    for tag in tags:
+        names += [f"{tag}_overlap.dat", f"{tag}_moments.dat", f"{tag}_glass_observables.dat",
+                  f"{tag}_sample_x2.dat"]
+    if sparse:
+        names.append("scatter_q_qlink.dat")
+    else:
+        assert not os.path.exists(tmp_path / "gpu" / "link_overlap.dat")
+    multi = sorted(f for f in os.listdir(refdir[0]) if f.startswith("multi_overlap_T"))
+    assert len(multi) == 4
+    names += multi
+    differ = [n for n in names if open(tmp_path / "gpu" / n).read() != open(os.path.join(refdir[0], n)).read()]
+    assert not differ, differ
