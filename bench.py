@@ -22,6 +22,15 @@ Lines (rank 0, one JSON line):
 
 Multi-GPU: one process per GPU (torchrun); every rank runs its own 256
 samples (weak scaling, no data-path collective); time is the max over ranks.
+
+--workload learned (not the default line): the learned-proposal PT
+configuration (dense N=64, uniform FMC gamma=0.1, 24 temperatures geometric
+in [0.2, 1.6], 4 replicas each, 64 samples): plain PT with recording, GPU
+training of the proposal network, plain equilibration, then interleaved
+ABBA blocks of each proposal at its autotuned block shape, reporting
+tau_int of E and q and the tau_int-corrected independent samples per second
+at slot 19 (T = 0.28714, the grid point nearest 0.3) for both
+(cuda_pspin_b200.learned_study).
 """
 from __future__ import annotations
 
@@ -327,6 +336,46 @@ def cpu_port_rate(args, sample_classes=True):
     return moves / sweep_s, threads, t_class
 
 
+def run_learned(args, rank, world):
+    """The learned-proposal configuration on one GPU (rank 0; the other ranks
+    exit): one JSON line with both proposals' tau_int and independent
+    samples per second at slot 19."""
+    if rank != 0:
+        return 0
+    import torch
+    from cuda_pspin_b200 import learned_study
+    torch.cuda.set_device(0)
+    study_args = argparse.Namespace(
+        N=64, samples=64, NT=NT, nrep=NREP_T, gamma=0.1, Tmin=TMIN, Tmax=TMAX, slot=19, seed0=42,
+        train_sweeps=1 << 14, equilibrate=args.equilibrate, measure_sweeps=1 << 14, blocks=16,
+        capacity=1 << 22, record_prob=0.01, train_steps=3000, batch=8192, lr=2e-3, net_seed=1, out="")
+    clocks = ClockSampler(0)
+    clocks.start()
+    res = learned_study.run(study_args)
+    clk = clocks.stop()
+    p, l = res["plain"], res["learned"]
+    keep = ("tau_E", "tau_E_err", "tau_q", "tau_q_err", "sweeps_per_s", "indep_E_per_s", "indep_q_per_s",
+            "E_per_N", "E_per_N_err", "acceptance_all_T")
+    line = {"metric": "tau_int-corrected independent E samples/s at T=0.28714 (slot 19)",
+            "value": l["indep_E_per_s"], "unit": "samples/s", "n_gpus": 1, "steps": study_args.blocks,
+            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (FP64 running energy; BF16 network weights, FP32 accumulate)", "data": "synthetic",
+            "config": {"workload": "learned-proposal PT: 64 samples, dense N=64, uniform FMC gamma=0.1, NT=24 "
+                                   "geometric [0.2,1.6], nrep=4, exchange every sweep",
+                       "train_sweeps": study_args.train_sweeps, "equilibrate_sweeps": study_args.equilibrate,
+                       "measure_sweeps_per_proposal": study_args.measure_sweeps,
+                       "blocks_per_proposal": study_args.blocks, "block_shapes": res["block_shapes"]},
+            "plain": {k: p[k] for k in keep}, "learned": {k: l[k] for k in keep},
+            "gain_E": res["gain_E"], "gain_q": res["gain_q"], "gain_q2": res["gain_q2"],
+            "E_learned_minus_plain": res["E_diff_mean"], "E_diff_err": res["E_diff_err"],
+            "E_diff_sigma": res["E_diff_sigma"],
+            "plain_block_means_first_last": [res["plain_block_means"][0], res["plain_block_means"][-1]],
+            "training": {k: res["training"][k] for k in ("records_seen", "train_s", "loss_start", "loss_end")},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -339,6 +388,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default="", help="W,C: warps per CTA, CTAs per replica block (skips the autotuner; "
                                                 "for profiling a fixed kernel shape)")
+    ap.add_argument("--workload", default="batched", choices=["batched", "learned"])
+    ap.add_argument("--equilibrate", type=int, default=1 << 15,
+                    help="learned workload: plain PT sweeps between training and measuring")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -370,6 +422,9 @@ def main():
                 "e2e": {"value": v, "unit": "pair-moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
+
+    if args.workload == "learned":
+        return run_learned(args, rank, world)
 
     import torch
     dist = None

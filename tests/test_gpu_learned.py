@@ -309,6 +309,9 @@ def test_observer_series_matches_state(ps):
 
 
 def _energy_series(ps, c, proposal, trained_w, nsweeps, burn):
+    """<E>/N with its error, tau_int(E) and the sweep kernel's seconds per
+    sweep (CUDA events around one launch of 200 sweeps)."""
+    import torch
     from cuda_pspin_b200 import tau as T
     with ps.Engine(c, ps.PSPIN_DENSE, ps.make_options(resync_every=256)) as eng:
         eng.learn_init(seed=1, capacity=16)
@@ -321,14 +324,28 @@ def _energy_series(ps, c, proposal, trained_w, nsweeps, burn):
         for _ in range(nsweeps):
             eng.sweep(1)
             xs.append(eng.get_results()[0].copy())
+        st = torch.cuda.ExternalStream(eng.stream_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        eng.sweep(20)
+        e0.record(st)
+        eng.sweep(200)
+        e1.record(st)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) * 1e-3 / 200
     x = np.array(xs).T / c.N                       # chains x n
     t = T.tau_int(x)
-    return x.mean(), np.sqrt(2 * t.tau * x.var() / x.size), t.tau
+    return x.mean(), np.sqrt(2 * t.tau * x.var() / x.size), t.tau, sec
 
 
 @pytest.mark.parametrize("T_", [0.4, 1.0])
 def test_learned_chain_matches_plain_energy(ps, T_):
-    """<E>/N of a trained learned chain equals the plain chain's (beta > 0)."""
+    """<E>/N of a trained learned chain equals the plain chain's (beta > 0)
+    within 2 sigma; at the low temperature the learned move decorrelates E at
+    least twice as fast per sweep and delivers more tau_int-corrected
+    independent samples per second of kernel time than the plain move (the
+    plain move timed on the same two-pass kernel shape and its own one-pass
+    kernel alike would only strengthen this: its one-pass kernel is
+    compared)."""
     N = 8
     c = ps.default_config(N=N, nrep=256, seed=13, fmc_mode=0, T=T_)
     with ps.Engine(c) as eng:
@@ -338,8 +355,14 @@ def test_learned_chain_matches_plain_energy(ps, T_):
         eng.sweep(300)
         eng.learn_train(400, 4096, 3e-3)
         w = eng.learn_params()
-    ep, sp, tp = _energy_series(ps, c, ps.PROPOSAL_PLAIN, None, 1500, 300)
-    el, sl, tl = _energy_series(ps, c, ps.PROPOSAL_LEARNED, w, 1500, 300)
+    ep, sp, tp, secp = _energy_series(ps, c, ps.PROPOSAL_PLAIN, None, 1500, 300)
+    el, sl, tl, secl = _energy_series(ps, c, ps.PROPOSAL_LEARNED, w, 1500, 300)
     z = (el - ep) / np.hypot(sp, sl)
-    print(f"T={T_} plain {ep:.5f}+-{sp:.5f} tau {tp:.2f}  learned {el:.5f}+-{sl:.5f} tau {tl:.2f}  z={z:.2f}")
-    assert abs(z) < 4.0
+    gain = (tp / tl) * (secp / secl)        # independent E samples per second, learned / plain
+    print(f"T={T_} plain {ep:.5f}+-{sp:.5f} tau {tp:.2f} {secp * 1e6:.1f} us/sweep  learned {el:.5f}+-{sl:.5f} "
+          f"tau {tl:.2f} {secl * 1e6:.1f} us/sweep  z={z:.2f}  tau ratio {tp / tl:.2f}  "
+          f"tau-corrected samples/s gain {gain:.2f}")
+    assert abs(z) < 2.0
+    if T_ < 0.5:
+        assert tp / tl >= 2.0
+        assert gain > 1.0
