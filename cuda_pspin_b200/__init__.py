@@ -66,7 +66,7 @@ class Options(ctypes.Structure):
                 ("quiet", ctypes.c_int), ("generic_lists", ctypes.c_int), ("graph_steps", ctypes.c_int),
                 ("resync_method", ctypes.c_int), ("cluster_size", ctypes.c_int),
                 ("wait_limit_clocks", ctypes.c_int), ("test_stall_move", ctypes.c_int),
-                ("reserved", ctypes.c_int * 1)]
+                ("disorder_stream", ctypes.c_int)]
 
 
 class Info(ctypes.Structure):
@@ -201,8 +201,10 @@ def parse_args(argv: list[str]) -> SimConfig:
 def make_options(init_exact: bool = False, resync_every: int = 0, warps_per_unit: int = 0,
                  trace: tuple[int, int, int] | None = None, quiet: bool = True,
                  generic_lists: bool = False, graph_steps: int = 0, resync_method: int = 0,
-                 cluster_size: int = 0, wait_limit_clocks: int = 0, test_stall_move: int = 0) -> Options:
+                 cluster_size: int = 0, wait_limit_clocks: int = 0, test_stall_move: int = 0,
+                 disorder_stream: bool = False) -> Options:
     o = Options()
+    o.disorder_stream = int(disorder_stream)
     o.cluster_size = int(cluster_size)
     o.wait_limit_clocks = int(wait_limit_clocks)
     o.test_stall_move = int(test_stall_move)

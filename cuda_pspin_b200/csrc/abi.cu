@@ -509,6 +509,22 @@ static void decode_q(int64_t q, int& i, int& j, int& k, int& l) {
 // mc_sparse.cu:477-537 without the dense temporaries: survivors are counted
 // per (l,k) block on the device and the partial Fisher-Yates shuffle runs on
 // a virtual array whose entries are located by rank.
+// Standard normal of quartet q for the streamed sparse set-up: Philox4x32-10
+// (rng.cuh) keyed by splitmix64 of the coupling seed, counter (q, TAG_G4),
+// two 53-bit uniforms u1 in (0, 1], u2 in [0, 1) and the Box-Muller transform
+// z = sqrt(-2 ln u1) cos(2 pi u2) (Box & Muller, Ann. Math. Statist. 29, 610,
+// 1958).  Host arithmetic; independent of every other quartet's draw.
+static double quartet_normal(uint64_t seed, int64_t q) {
+    uint64_t st = seed;
+    const uint64_t key = splitmix64(st);
+    const U4 w = philox4x32_10(U4{(uint32_t)q, (uint32_t)((uint64_t)q >> 32), 0u, 0x67346e72u},
+                               (uint32_t)key, (uint32_t)(key >> 32));
+    const uint64_t m1 = ((uint64_t)w.x << 32) | w.y, m2 = ((uint64_t)w.z << 32) | w.w;
+    const double u1 = ((double)(m1 >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+    const double u2 = (double)(m2 >> 11) * (1.0 / 9007199254740992.0);
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+}
+
 static int setup_sparse_quartets(pspin_state* s, SampleHost& h, std::vector<QuartetRec>& qs) {
     const pspin_config& c = h.cfg;
     const int N = c.N;
@@ -579,16 +595,21 @@ static int setup_sparse_quartets(pspin_state* s, SampleHost& h, std::vector<Quar
     }
     // coupling values: the same single cuRAND call as the reference's dense
     // temporary (mc_sparse.cu:424, disorder.cu:93-106), gathered at the
-    // selected quartets
+    // selected quartets; or, with disorder_stream, one counter-based normal
+    // per selected quartet (no C(N,4)-sized memory, not the reference's values)
     std::vector<double> raw(ns);
-    if (ns > 0) {
+    if (ns > 0 && s->opt.disorder_stream) {
+        for (int t = 0; t < ns; t++) raw[t] = quartet_normal(c.seed + 2000 + 12345, selq[t]);
+    } else if (ns > 0) {
         double* d_nrm = nullptr;
         int64_t* d_q = nullptr;
         double* d_out = nullptr;
         int rc = dalloc(&d_nrm, 2 * (size_t)nq);
         if (rc != PSPIN_OK)
             return fail(PSPIN_ERR_ALLOC,
-                        "sparse set-up needs the cuRAND stream of 2*C(N,4) = %lld doubles on the device: %s",
+                        "sparse set-up needs the cuRAND stream of 2*C(N,4) = %lld doubles on the device (%s); "
+                        "options.disorder_stream = 1 draws the selected couplings without it (same law, "
+                        "not the reference's values)",
                         (long long)(2 * nq), g_err.c_str());
         rc = dalloc(&d_q, ns);
         if (rc == PSPIN_OK) rc = dalloc(&d_out, ns);
@@ -2189,7 +2210,7 @@ extern "C" int pspin_learn_loss_grad(pspin_state* s, const float* records, int n
 // (which keys the pair and move streams), the resync phase, the PT state and
 // the learned network with its Adam moments.  Loading checks that the handle
 // was built from the same configurations (variant, N, replicas, seed, FMC).
-static const char kCkMagic[8] = {'P', 'S', 'P', 'I', 'N', 'C', 'K', '1'};
+static const char kCkMagic[8] = {'P', 'S', 'P', 'I', 'N', 'C', 'K', '2'};
 
 namespace {
 struct CkFile {
@@ -2232,6 +2253,7 @@ extern "C" int pspin_checkpoint_save(pspin_state* s, const char* path) {
     CK(cudaMemcpy(&counter, s->d_sweep_counter, sizeof(counter), cudaMemcpyDeviceToHost));
     f.put(kCkMagic, sizeof(kCkMagic));
     f.put((int32_t)s->variant);
+    f.put((int32_t)s->opt.disorder_stream);   // which couplings the chain ran on
     f.put((int32_t)s->S);
     f.put((int64_t)s->R_tot);
     f.put((int64_t)s->spin_total);
@@ -2291,11 +2313,13 @@ extern "C" int pspin_checkpoint_load(pspin_state* s, const char* path) {
     char magic[8];
     f.get(magic, sizeof(magic));
     if (!f.ok || std::memcmp(magic, kCkMagic, sizeof(magic)) != 0) return fail(PSPIN_ERR_ARG, "%s is not a checkpoint", path);
-    int32_t variant = 0, S = 0;
+    int32_t variant = 0, dstream = 0, S = 0;
     int64_t R_tot = 0, spin_total = 0;
-    f.get(variant); f.get(S); f.get(R_tot); f.get(spin_total);
-    if (!f.ok || variant != s->variant || S != s->S || R_tot != s->R_tot || spin_total != s->spin_total)
-        return fail(PSPIN_ERR_ARG, "checkpoint does not match this handle (variant, samples or replicas)");
+    f.get(variant); f.get(dstream); f.get(S); f.get(R_tot); f.get(spin_total);
+    if (!f.ok || variant != s->variant || S != s->S || R_tot != s->R_tot || spin_total != s->spin_total ||
+        dstream != s->opt.disorder_stream)
+        return fail(PSPIN_ERR_ARG,
+                    "checkpoint does not match this handle (variant, coupling source, samples or replicas)");
     for (const SampleHost& h : s->hs) {
         int32_t N = 0, R = 0, fmc = 0;
         uint64_t seed = 0;

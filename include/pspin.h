@@ -107,7 +107,16 @@ typedef struct pspin_options {
                             of the ring-fed sweep kernels wait, at move k-1
                             of each launch, on a barrier that nothing
                             completes, so the bounded wait runs out; 0: off */
-    int reserved[1];
+    int disorder_stream; /* sparse set-up: 0 (default) the reference's couplings
+                            bit for bit, from its single cuRAND call of
+                            2*C(N,4) normals (2*8*C(N,4) bytes on the device:
+                            45 GB at N=512, beyond the device near N=700);
+                            1: each selected quartet's coupling from its own
+                            counter-based normal (Philox4x32-10 + Box-Muller),
+                            the same Gaussian law but not the reference's
+                            values, with no C(N,4)-sized memory.  The FMC
+                            survivors and the quartet selection are the
+                            reference's either way. */
 } pspin_options;
 
 typedef struct pspin_info {
