@@ -56,6 +56,9 @@ cudaError_t launch_sample_index(int* idx, int n, unsigned long long filled, uint
                                 cudaStream_t st);
 constexpr int kMlpParamsHost = 6426, kRecordFloatsHost = 11, kSaveFloatsHost = 8 + 4 * 64 + 26;
 cudaError_t dev_fmc_mask(uint8_t* mask, const double* omega, int N, double gamma, cudaStream_t st);
+cudaError_t launch_cube_normalize_many(double* all, int N, int nsamples, cudaStream_t st);
+cudaError_t launch_cube_walk(float2* a, int N, int sweeps, int save_freq, uint64_t move_key, uint64_t pair_key,
+                             double* traj, int max_saved, int* n_saved, cudaStream_t st);
 cudaError_t dev_survivor_counts(unsigned long long* counts, const double* omega, int N, double gamma, cudaStream_t st);
 cudaError_t dev_popcount(const uint8_t* mask, int64_t n, unsigned long long* out, cudaStream_t st);
 cudaError_t dev_g4_real(const double* normals, double* g4, int64_t n, double sigma, double mean, cudaStream_t st);
@@ -2464,6 +2467,70 @@ extern "C" int pspin_fmc_mask(int N, const double* omega, double gamma, uint8_t*
     if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "fmc mask: %s", cudaGetErrorString(e));
     if (n_active) *n_active = (int64_t)cnt;
     return PSPIN_OK;
+}
+
+// ------------------------------------------------------------------ smoothed cube
+// smoothed_cube.cu:330-352: nsamples configurations of N amplitudes from one
+// cuRAND Philox call of 2 N nsamples normals (seed), each scaled onto
+// sum |a|^4 = N on the device; out [nsamples][N][2].
+extern "C" int pspin_cube_samples(int N, int nsamples, uint64_t seed, double* out) {
+    if (N < 2 || nsamples < 1 || !out) return fail(PSPIN_ERR_ARG, "need N >= 2, nsamples >= 1 and an output");
+    const size_t n = 2 * (size_t)N * nsamples;
+    double* d = nullptr;
+    TRY(dalloc(&d, n));
+    int rc = curand_normals(seed, n, d, 0);
+    cudaError_t e = cudaSuccess;
+    if (rc == PSPIN_OK) e = launch_cube_normalize_many(d, N, nsamples, 0);
+    if (rc == PSPIN_OK && e == cudaSuccess) e = cudaMemcpy(out, d, n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (rc != PSPIN_OK) return rc;
+    if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "cube samples: %s", cudaGetErrorString(e));
+    return PSPIN_OK;
+}
+
+// The free walk of smoothed_cube.cu:74-119 on the engine's cube move: the
+// start is the reference's init_spins_cube(seed + 9999) (spins_sparse.cu:
+// 63-80: cuRAND normals, the shared-memory tree normalisation), rounded to
+// FP32; `sweeps` sweeps of N/2 always-accepted moves from the engine's
+// streams keyed by seed + 12345; traj [max_saved][N][2] gets the state
+// before the walk and after every save_freq-th sweep, *n_saved the count.
+extern "C" int pspin_cube_walk(int N, int sweeps, int save_freq, uint64_t seed, double* traj, int max_saved,
+                               int* n_saved) {
+    if (N < 2 || sweeps < 0 || save_freq < 1 || max_saved < 1 || !traj || !n_saved)
+        return fail(PSPIN_ERR_ARG, "need N >= 2, sweeps >= 0, save_freq >= 1 and an output");
+    double* d_nrm = nullptr;
+    TRY(dalloc(&d_nrm, 2 * (size_t)N));
+    std::vector<double> a0(2 * (size_t)N);
+    int rc = curand_normals(seed + 9999, 2 * (size_t)N, d_nrm, 0);
+    cudaError_t e = cudaSuccess;
+    if (rc == PSPIN_OK) e = cudaMemcpy(a0.data(), d_nrm, a0.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d_nrm);
+    if (rc != PSPIN_OK) return rc;
+    if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "cube walk: %s", cudaGetErrorString(e));
+    normalize_host(a0.data(), N, 1, 0);
+    std::vector<float2> af(N);
+    for (int k = 0; k < N; k++) af[k] = make_float2((float)a0[2 * k], (float)a0[2 * k + 1]);
+    uint64_t st = seed + 12345;
+    const uint64_t move_key = splitmix64(st), pair_key = splitmix64(st);
+    float2* d_a = nullptr;
+    double* d_t = nullptr;
+    int* d_n = nullptr;
+    rc = dalloc(&d_a, N);
+    if (rc == PSPIN_OK) rc = dalloc(&d_t, 2 * (size_t)N * max_saved);
+    if (rc == PSPIN_OK) rc = dalloc(&d_n, 1);
+    if (rc == PSPIN_OK) {
+        e = cudaMemcpy(d_a, af.data(), N * sizeof(float2), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = launch_cube_walk(d_a, N, sweeps, save_freq, move_key, pair_key, d_t, max_saved, d_n, 0);
+        if (e == cudaSuccess) e = cudaMemcpy(n_saved, d_n, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(traj, d_t, 2 * (size_t)N * std::min(*n_saved, max_saved) * sizeof(double),
+                           cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(PSPIN_ERR_CUDA, "cube walk: %s", cudaGetErrorString(e));
+    }
+    cudaFree(d_a);
+    cudaFree(d_t);
+    cudaFree(d_n);
+    return rc;
 }
 
 extern "C" int pspin_quartet_roundtrip(int N, int64_t* n_fail) {

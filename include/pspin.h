@@ -371,6 +371,23 @@ int  pspin_quartet_roundtrip(int N, int64_t* n_fail);
 int  pspin_fmc_survivors_static(int N, const double* omega, double gamma, int64_t* counts,
                                 void* stream);
 
+/* ---- the smoothed-cube check (smoothed_cube.cu) ----------------------- */
+/* nsamples configurations of N amplitudes on sum |a|^4 = N: one cuRAND
+ * Philox call of 2 N nsamples normals from seed, each configuration scaled
+ * by (N / sum |a|^4)^(1/4) on the device (smoothed_cube.cu:330-352); out
+ * [nsamples][N][2]. */
+int  pspin_cube_samples(int N, int nsamples, uint64_t seed, double* out);
+/* The free walk of smoothed_cube.cu:74-119 (no Hamiltonian, every move
+ * accepted) with the engine's FP32 cube move: start init_spins_cube(seed +
+ * 9999) (spins_sparse.cu:63-80), N/2 moves per sweep (the pair (0,1) when
+ * N = 2), streams keyed by seed + 12345; traj [max_saved][N][2] holds the
+ * start and the state after every save_freq-th sweep, *n_saved their number.
+ * The walk is the engine's, so its points are not the reference's; its law
+ * (|a_i|^4 / (|a_i|^4 + |a_j|^4) uniform after a move) and the constraint
+ * are. */
+int  pspin_cube_walk(int N, int sweeps, int save_freq, uint64_t seed, double* traj, int max_saved,
+                     int* n_saved);
+
 /* ---- measurement (no reference counterpart) --------------------------- */
 /* The CUDA stream (cudaStream_t) all of this handle's work runs on. */
 void* pspin_stream(pspin_state* s);
