@@ -136,6 +136,10 @@ def load_library() -> ctypes.CDLL:
         "pspin_fy_downsample": (ctypes.c_int, [ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_uint32,
                                                vp, vp]),
         "pspin_tau_e": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, vp, vp]),
+        "pspin_shard_samples": (ctypes.c_int, [ctypes.c_int, vp, vp, ctypes.c_int, vp]),
+        "pspin_cube_samples": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, vp]),
+        "pspin_cube_walk": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, vp,
+                                           ctypes.c_int, vp]),
         "pspin_set_proposal": (ctypes.c_int, [vp, ctypes.c_int]),
         "pspin_observe_init": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
         "pspin_autotune": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp]),
@@ -553,6 +557,16 @@ def fmc_mask(N: int, omega, gamma: float):
     n = ctypes.c_int64(0)
     _check(load_library().pspin_fmc_mask(N, _ptr(w), float(gamma), _ptr(m), ctypes.byref(n)))
     return m, n.value
+
+
+def shard_samples(Ns, Rs, nshards: int) -> np.ndarray:
+    """Shard of every sample (pspin_shard_samples: cost N^4 R, largest first
+    to the least-loaded shard); the same on every rank."""
+    N = np.ascontiguousarray(Ns, np.int32)
+    R = np.ascontiguousarray(np.broadcast_to(np.asarray(Rs, np.int32), N.shape), np.int32)
+    out = np.zeros(len(N), np.int32)
+    _check(load_library().pspin_shard_samples(len(N), _ptr(N), _ptr(R), int(nshards), _ptr(out)))
+    return out
 
 
 def fp32_peak_tflops() -> float:

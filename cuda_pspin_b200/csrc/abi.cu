@@ -2469,6 +2469,35 @@ extern "C" int pspin_fmc_mask(int N, const double* omega, double gamma, uint8_t*
     return PSPIN_OK;
 }
 
+// ------------------------------------------------------------------ multi-GPU sharding
+// Longest-processing-time bin packing of independent samples over shards
+// (GPUs): costs N^4 R (one sweep's field work: N/2 moves over site lists of
+// ~N^3 terms, for R replicas), taken largest first (ties by index) and each
+// given to the least-loaded shard (ties by shard index).  Deterministic, so
+// every rank computes the same assignment without communicating.
+extern "C" int pspin_shard_samples(int n_samples, const int* N, const int* R, int nshards, int* shard_of) {
+    if (n_samples < 0 || nshards < 1 || (n_samples > 0 && (!N || !R || !shard_of)))
+        return fail(PSPIN_ERR_ARG, "pspin_shard_samples: bad arguments");
+    std::vector<int> order(n_samples);
+    std::vector<double> cost(n_samples);
+    for (int k = 0; k < n_samples; k++) {
+        if (N[k] < 1 || R[k] < 1) return fail(PSPIN_ERR_ARG, "pspin_shard_samples: N and R must be >= 1");
+        const double n = (double)N[k];
+        cost[k] = n * n * n * n * (double)R[k];
+        order[k] = k;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<double> load(nshards, 0.0);
+    for (int k : order) {
+        int best = 0;
+        for (int r = 1; r < nshards; r++)
+            if (load[r] < load[best]) best = r;
+        shard_of[k] = best;
+        load[best] += cost[k];
+    }
+    return PSPIN_OK;
+}
+
 // ------------------------------------------------------------------ smoothed cube
 // smoothed_cube.cu:330-352: nsamples configurations of N amplitudes from one
 // cuRAND Philox call of 2 N nsamples normals (seed), each scaled onto

@@ -13,6 +13,9 @@
 // Extension (no reference counterpart): -batch K runs K disorder samples
 // (labels label..label+K-1, seeds seed..seed+K-1) in one batched engine and
 // writes one data directory per sample, as K separate runs would.
+// -shard r/n runs only the samples of those K that pspin_shard_samples gives
+// to shard r of n (one process per GPU, with -dev), so n processes together
+// write the K directories of the unsharded run, file for file.
 #include "common.h"
 
 #include <sys/stat.h>
@@ -27,6 +30,19 @@
 #include <vector>
 
 namespace {
+
+// "-shard r/n": r in [0, n); the indices of the K samples of shard r
+bool parse_shard(const char* a, int& r, int& n) {
+    return sscanf(a, "%d/%d", &r, &n) == 2 && n >= 1 && r >= 0 && r < n;
+}
+
+std::vector<int> shard_indices(int K, int N, int R, int r, int n) {
+    std::vector<int> Ns(K, N), Rs(K, R), of(K, 0), mine;
+    if (n > 1 && pspin_shard_samples(K, Ns.data(), Rs.data(), n, of.data()) != PSPIN_OK) return mine;
+    for (int k = 0; k < K; k++)
+        if (of[k] == r) mine.push_back(k);
+    return mine;
+}
 
 // config.h:50-57
 void fmt_param(char* buf, int sz, double v) {
@@ -83,7 +99,7 @@ int pt_main(int argc, char** argv, int variant) {
     const bool sparse = variant == PSPIN_SPARSE;
     // parallel_tempering.cu:34-56: PT flags, the rest for parse_args
     double Tmax = -1.0, Tmin = -1.0;
-    int NT = -1, pt_freq = -1, log_temp = 0, batch = 1;
+    int NT = -1, pt_freq = -1, log_temp = 0, batch = 1, shard = 0, nshards = 1;
     std::vector<char*> rest;
     rest.push_back(argv[0]);
     for (int i = 1; i < argc; i++) {
@@ -93,14 +109,20 @@ int pt_main(int argc, char** argv, int variant) {
         else if (!strcmp(argv[i], "-pt_freq") && i + 1 < argc) pt_freq = atoi(argv[++i]);
         else if (!strcmp(argv[i], "-log_temp")) log_temp = 1;
         else if (!strcmp(argv[i], "-batch") && i + 1 < argc) batch = atoi(argv[++i]);
-        else rest.push_back(argv[i]);
+        else if (!strcmp(argv[i], "-shard") && i + 1 < argc) {
+            if (!parse_shard(argv[++i], shard, nshards)) {
+                fprintf(stderr, "Error: -shard takes r/n with 0 <= r < n\n");
+                return 1;
+            }
+        } else rest.push_back(argv[i]);
     }
     if (Tmax < 0 || Tmin < 0 || NT < 2 || pt_freq < 1) {
         fprintf(stderr, "%s requires: -Tmax t -Tmin t -NT nt -pt_freq p\n",
                 sparse ? "Sparse PT" : "Parallel Tempering");
         fprintf(stderr, "Usage: %s -N n -Tmax t -Tmin t -NT nt -pt_freq p -iter k "
                         "[-nrep n] [-J j] [-seed s] [-save_freq f] [-label l] [-dev d] "
-                        "[-fmc 0|1|2] [-gamma g] [-verbose [0|1|2]] [-log_temp] [-batch K]\n", argv[0]);
+                        "[-fmc 0|1|2] [-gamma g] [-verbose [0|1|2]] [-log_temp] [-batch K] [-shard r/n]\n",
+                argv[0]);
         return 1;
     }
     if (Tmin > Tmax) {
@@ -132,13 +154,20 @@ int pt_main(int argc, char** argv, int variant) {
     }
 
     const int label0 = (cfg.label >= 0) ? cfg.label : 0;
+    const bool labelled = batch > 1 || cfg.label >= 0;
+    const std::vector<int> idx = shard_indices(batch, cfg.N, total_replicas, shard, nshards);
+    if (idx.empty()) {
+        printf("  shard %d/%d holds none of the %d samples\n", shard, nshards, batch);
+        return 0;
+    }
+    batch = (int)idx.size();
     std::vector<pspin_config> cfgs(batch, cfg);
     std::vector<SampleFiles> files(batch);
     mkdir("data", 0755);
     for (int k = 0; k < batch; k++) {
-        cfgs[k].seed = cfg.seed + (uint64_t)k;
-        cfgs[k].label = (batch > 1 || cfg.label >= 0) ? label0 + k : cfg.label;
-        const int label = label0 + k;
+        cfgs[k].seed = cfg.seed + (uint64_t)idx[k];
+        cfgs[k].label = labelled ? label0 + idx[k] : cfg.label;
+        const int label = label0 + idx[k];
         char datadir[256];
         make_run_dir(datadir, sizeof(datadir), "data", sparse ? "PTS" : "PT", cfg.N, cfg.alpha, cfg.J, cfg.J0,
                      cfg.alpha0, NT, nrep_per_temp, label);
@@ -350,7 +379,7 @@ int pt_main(int argc, char** argv, int variant) {
 int sa_main(int argc, char** argv) {
     // simulated_annealing.cu:32-70: SA flags, the rest for parse_args
     double Tmax = -1.0, Tmin = -1.0;
-    int ntemp = -1, batch = 1;
+    int ntemp = -1, batch = 1, shard = 0, nshards = 1;
     std::vector<char*> rest;
     rest.push_back(argv[0]);
     for (int i = 1; i < argc; i++) {
@@ -358,13 +387,18 @@ int sa_main(int argc, char** argv) {
         else if (!strcmp(argv[i], "-Tmin") && i + 1 < argc) Tmin = atof(argv[++i]);
         else if (!strcmp(argv[i], "-ntemp") && i + 1 < argc) ntemp = atoi(argv[++i]);
         else if (!strcmp(argv[i], "-batch") && i + 1 < argc) batch = atoi(argv[++i]);
-        else rest.push_back(argv[i]);
+        else if (!strcmp(argv[i], "-shard") && i + 1 < argc) {
+            if (!parse_shard(argv[++i], shard, nshards)) {
+                fprintf(stderr, "Error: -shard takes r/n with 0 <= r < n\n");
+                return 1;
+            }
+        } else rest.push_back(argv[i]);
     }
     if (Tmax < 0 || Tmin < 0 || ntemp < 1) {
         fprintf(stderr, "Simulated Annealing requires: -Tmax tmax -Tmin tmin -ntemp nt\n");
         fprintf(stderr, "Usage: %s -N n -Tmax tmax -Tmin tmin -ntemp nt -iter k "
                         "[-nrep n] [-J j] [-seed s] [-save_freq f] [-label l] [-dev d] "
-                        "[-fmc 0|1|2] [-gamma g] [-verbose [0|1|2]] [-batch K]\n", argv[0]);
+                        "[-fmc 0|1|2] [-gamma g] [-verbose [0|1|2]] [-batch K] [-shard r/n]\n", argv[0]);
         return 1;
     }
     if (Tmin > Tmax) {
@@ -390,15 +424,21 @@ int sa_main(int argc, char** argv) {
 
     // one data directory per sample, data/SA_N{N}_NR{nrep}_S{label} (:83-100)
     const int label0 = (cfg.label >= 0) ? cfg.label : 0;
+    const std::vector<int> idx = shard_indices(batch, N, nrep, shard, nshards);
+    if (idx.empty()) {
+        printf("  shard %d/%d holds none of the %d samples\n", shard, nshards, batch);
+        return 0;
+    }
+    batch = (int)idx.size();
     std::vector<pspin_config> cfgs(batch, cfg);
     std::vector<std::string> dirs(batch);
     std::vector<FILE*> fouts(batch, nullptr);
     mkdir("data", 0755);
     for (int k = 0; k < batch; k++) {
-        cfgs[k].seed = cfg.seed + (uint64_t)k;
-        cfgs[k].label = label0 + k;
+        cfgs[k].seed = cfg.seed + (uint64_t)idx[k];
+        cfgs[k].label = label0 + idx[k];
         char datadir[256];
-        snprintf(datadir, sizeof(datadir), "data/SA_N%d_NR%d_S%d", N, nrep, label0 + k);
+        snprintf(datadir, sizeof(datadir), "data/SA_N%d_NR%d_S%d", N, nrep, label0 + idx[k]);
         mkdir(datadir, 0755);
         dirs[k] = datadir;
         mkdir((dirs[k] + "/configs").c_str(), 0755);

@@ -371,6 +371,13 @@ int  pspin_quartet_roundtrip(int N, int64_t* n_fail);
 int  pspin_fmc_survivors_static(int N, const double* omega, double gamma, int64_t* counts,
                                 void* stream);
 
+/* ---- multi-GPU sharding (no reference counterpart; the reference runs
+ * one process per sample, scan_samples_pt:145-169) ---------------------- */
+/* Assigns n_samples independent samples (sizes N[k], replicas R[k]) to
+ * nshards GPUs by cost N^4 R, largest first to the least-loaded shard.
+ * Deterministic: every rank computes the same shard_of[n_samples] alone. */
+int  pspin_shard_samples(int n_samples, const int* N, const int* R, int nshards, int* shard_of);
+
 /* ---- the smoothed-cube check (smoothed_cube.cu) ----------------------- */
 /* nsamples configurations of N amplitudes on sum |a|^4 = N: one cuRAND
  * Philox call of 2 N nsamples normals from seed, each configuration scaled

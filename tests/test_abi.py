@@ -95,3 +95,19 @@ def test_host_exchange_matches_oracle(ps, orc):
 
 def orc_srand(orc, seed):
     return int(orc.lib().orc_srand48_state(seed))
+
+
+def test_shard_samples_lpt(ps):
+    """pspin_shard_samples: deterministic, complete, and within one largest
+    cost of a perfect balance; equal samples go round robin."""
+    rng = np.random.default_rng(3)
+    Ns = rng.choice([24, 32, 48, 64], size=101)
+    for n in (1, 2, 5, 8):
+        of = ps.shard_samples(Ns, 96, n)
+        assert np.array_equal(of, ps.shard_samples(Ns, 96, n))
+        assert set(of.tolist()) <= set(range(n))
+        loads = np.array([np.sum(Ns[of == r].astype(float) ** 4) for r in range(n)])
+        assert loads.max() - loads.min() <= 64.0 ** 4
+    assert ps.shard_samples([16] * 7, 4, 3).tolist() == [0, 1, 2, 0, 1, 2, 0]
+    with pytest.raises(ps.PspinError):
+        ps.shard_samples([16, 0], 4, 2)

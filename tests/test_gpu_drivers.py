@@ -284,3 +284,31 @@ def test_gpu_deeper_analysis_matches_analysis_pt(tmp_path, variant):
     names += multi
     differ = [n for n in names if open(tmp_path / "gpu" / n).read() != open(os.path.join(refdir[0], n)).read()]
     assert not differ, differ
+
+
+@pytest.mark.parametrize("prog,extra", [("pspin_pt", ["-Tmax", "1.6", "-Tmin", "0.3", "-NT", "4", "-log_temp",
+                                                     "-pt_freq", "1"]),
+                                        ("pspin_sa", ["-Tmax", "1.6", "-Tmin", "0.3", "-ntemp", "4"])])
+def test_sharded_driver_equals_unsharded(tmp_path, prog, extra):
+    """-batch 5 split over three processes with -shard r/3 (each would run
+    on its own GPU with -dev) writes the same five data directories as one
+    unsharded -batch 5 run, file for file (time.txt aside)."""
+    flags = ["-N", "12", "-nrep", "3", "-iter", "8" if prog == "pspin_sa" else "256", "-save_freq", "16",
+             "-seed", "5", "-label", "0", "-batch", "5", *extra]
+    one, split = tmp_path / "one", tmp_path / "split"
+    one.mkdir()
+    split.mkdir()
+    run([os.path.join(BIN, prog), *flags], one)
+    for r in range(3):
+        run([os.path.join(BIN, prog), *flags, "-shard", f"{r}/3"], split)
+    d1, d2 = sorted(os.listdir(one / "data")), sorted(os.listdir(split / "data"))
+    assert d1 == d2 and len(d1) == 5
+    for d in d1:
+        for root, _, fs in os.walk(one / "data" / d):
+            for f in fs:
+                if f == "time.txt":
+                    continue
+                rel = os.path.relpath(os.path.join(root, f), one / "data" / d)
+                a = open(os.path.join(root, f), "rb").read()
+                b = open(split / "data" / d / rel, "rb").read()
+                assert a == b, (d, rel)

@@ -38,6 +38,45 @@ def _worker(rank, world, port, q):
     dist.destroy_process_group()
 
 
+def _shard_worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    import cuda_pspin_b200 as ps
+    Ns, seeds = bench.workload(256, 0)                  # one fixed set of samples for all ranks
+    of = ps.shard_samples(Ns, 96, world)
+    mine = [int(k) for k in range(len(Ns)) if of[k] == rank]
+    gathered = [None] * world
+    dist.all_gather_object(gathered, mine)
+    dist.barrier()
+    if rank == 0:
+        q.put((gathered, Ns))
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_fixed_samples_shard_by_cost(world):
+    """A fixed set of samples of uneven N spread over `world` ranks by
+    pspin_shard_samples (no communication: every rank computes the same
+    assignment): every sample on exactly one rank, and the ranks' N^4 costs
+    within the largest single sample's cost of each other."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    gathered, Ns = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    allk = sorted(k for g in gathered for k in g)
+    assert allk == list(range(len(Ns)))
+    loads = [sum(Ns[k] ** 4 for k in g) for g in gathered]
+    assert max(loads) - min(loads) <= max(Ns) ** 4
+
+
 def test_sample_sharding_and_max_timing():
     world = 2
     ctx = mp.get_context("spawn")
