@@ -57,6 +57,11 @@ cudaError_t launch_sample_index(int* idx, int n, unsigned long long filled, uint
 constexpr int kMlpParamsHost = 6426, kRecordFloatsHost = 11, kSaveFloatsHost = 8 + 4 * 64 + 26;
 cudaError_t dev_fmc_mask(uint8_t* mask, const double* omega, int N, double gamma, cudaStream_t st);
 cudaError_t launch_cube_normalize_many(double* all, int N, int nsamples, cudaStream_t st);
+cudaError_t dev_g2_build(const double* normals, int N, const double* omega, double gamma, double* g2,
+                         unsigned long long* count, cudaStream_t st);
+cudaError_t dev_g2_scale(double* g2, long long n, double sigma, double mean, int shift, cudaStream_t st);
+cudaError_t dev_normalize_replicas(const double* nrm, int N, int R, int cube, int exact, float2* spins,
+                                   double* target, cudaStream_t st);
 cudaError_t launch_cube_walk(float2* a, int N, int sweeps, int save_freq, uint64_t move_key, uint64_t pair_key,
                              double* traj, int max_saved, int* n_saved, cudaStream_t st);
 cudaError_t dev_survivor_counts(unsigned long long* counts, const double* omega, int N, double gamma, cudaStream_t st);
@@ -350,62 +355,55 @@ static void omega_of(const pspin_config& c, std::vector<double>& w) {
 
 // g2 generation, FMC, survivor count, rescale, mean shift
 // (mc.cu:443-444, 465-478, 491-498; disorder.cu:57-91, 130-143)
+// g2 on the device (disorder.cu:45-80, 130-143, 191-197; mc.cu:436-502):
+// cuRAND normals (seed + 1000), real parts, symmetric copy, FMC filter and
+// survivor count (i <= j, the diagonal always survives), then sigma =
+// J2 sqrt(N / n) and the mean shift on the non-zero entries; the host keeps
+// a copy for the layouts.
 static int setup_g2(SampleHost& h, cudaStream_t st) {
     const pspin_config& c = h.cfg;
     const int N = c.N;
     const double J2 = (1.0 - c.alpha) * c.J, J20 = (1.0 - c.alpha0) * c.J0;
     h.g2re.assign((size_t)N * N, 0.0);
-    if (c.fmc_mode != 1) {
-        double* d = nullptr;
-        TRY(dalloc(&d, 2 * (size_t)N * N));
-        int rc = curand_normals(c.seed + 1000, 2 * (size_t)N * N, d, st);
-        std::vector<double> nrm(2 * (size_t)N * N);
-        if (rc == PSPIN_OK) {
-            cudaError_t e = cudaMemcpyAsync(nrm.data(), d, nrm.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) rc = fail(PSPIN_ERR_CUDA, "g2 copy: %s", cudaGetErrorString(e));
+    if (c.fmc_mode > 0) omega_of(c, h.omega);
+    else h.omega.clear();
+    if (c.fmc_mode == 1) {                 // comb: H2 fully killed
+        h.n_pairs_active = 0;
+        h.h2_active = 0;
+        return PSPIN_OK;
+    }
+    double *d = nullptr, *d_g2 = nullptr, *d_w = nullptr;
+    unsigned long long* d_cnt = nullptr;
+    int rc = dalloc(&d, 2 * (size_t)N * N);
+    if (rc == PSPIN_OK) rc = dalloc(&d_g2, (size_t)N * N);
+    if (rc == PSPIN_OK) rc = dalloc(&d_w, (size_t)N);
+    if (rc == PSPIN_OK) rc = dalloc(&d_cnt, 1);
+    if (rc == PSPIN_OK) rc = curand_normals(c.seed + 1000, 2 * (size_t)N * N, d, st);
+    unsigned long long cnt = 0;
+    if (rc == PSPIN_OK) {
+        cudaError_t e = cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st);
+        if (e == cudaSuccess && c.fmc_mode == 2)
+            e = cudaMemcpyAsync(d_w, h.omega.data(), N * sizeof(double), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = dev_g2_build(d, N, c.fmc_mode == 2 ? d_w : nullptr, c.gamma, d_g2, d_cnt, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess) {
+            h.n_pairs_active = c.fmc_mode == 2 ? (int64_t)cnt : (int64_t)N * (N + 1) / 2;
+            const double sigma = h.n_pairs_active > 0 ? J2 * std::sqrt((double)N / (double)h.n_pairs_active) : 1.0;
+            const double mean = (J20 != 0.0 && h.n_pairs_active > 0) ? J20 * (double)N / (double)h.n_pairs_active : 0.0;
+            e = dev_g2_scale(d_g2, (long long)N * N, sigma, mean, mean != 0.0 ? 1 : 0, st);
         }
-        cudaFree(d);
-        if (rc != PSPIN_OK) return rc;
-        // imag dropped, lower triangle copied from the upper one, diagonal kept
-        for (int i = 0; i < N; i++)
-            for (int j = 0; j < N; j++) {
-                const size_t src = (i > j) ? (size_t)j * N + i : (size_t)i * N + j;
-                h.g2re[(size_t)i * N + j] = nrm[2 * src];
-            }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h.g2re.data(), d_g2, (size_t)N * N * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = fail(PSPIN_ERR_CUDA, "g2 set-up: %s", cudaGetErrorString(e));
     }
-    if (c.fmc_mode > 0) {
-        omega_of(c, h.omega);
-        if (c.fmc_mode == 1) {
-            h.n_pairs_active = 0;
-        } else {
-            for (int i = 0; i < N; i++)
-                for (int j = i + 1; j < N; j++)
-                    if (std::fabs(h.omega[i] - h.omega[j]) > c.gamma) {
-                        h.g2re[(size_t)i * N + j] = 0.0;
-                        h.g2re[(size_t)j * N + i] = 0.0;
-                    }
-            int64_t n = 0;
-            for (int i = 0; i < N; i++)
-                for (int j = i; j < N; j++)
-                    if (h.g2re[(size_t)i * N + j] != 0.0) n++;
-            h.n_pairs_active = n;
-        }
-    } else {
-        h.omega.clear();
-        h.n_pairs_active = (int64_t)N * (N + 1) / 2;
-    }
-    if (h.n_pairs_active > 0) {
-        const double sigma = J2 * std::sqrt((double)N / (double)h.n_pairs_active);
-        for (double& v : h.g2re) v *= sigma;
-    }
-    if (J20 != 0.0 && h.n_pairs_active > 0) {
-        const double mean = J20 * (double)N / (double)h.n_pairs_active;
-        for (double& v : h.g2re)
-            if (v != 0.0) v += mean;
-    }
+    cudaFree(d);
+    cudaFree(d_g2);
+    cudaFree(d_w);
+    cudaFree(d_cnt);
     h.h2_active = h.n_pairs_active > 0 ? 1 : 0;
-    return PSPIN_OK;
+    return rc;
 }
 
 // spins.cu:27-69 (sphere) / spins_sparse.cu:28-61 (cube), on the host in
@@ -802,8 +800,6 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     // ---- disorder, spins, layouts
     std::vector<SiteLists> lists(n);
     std::vector<std::vector<Q64>> q64(n);
-    std::vector<std::vector<float2>> spins(n);
-    std::vector<std::vector<double>> targets(n);
     std::vector<std::vector<uint64_t>> keys(n);
     const bool timing = std::getenv("PSPIN_SETUP_TIMING") != nullptr;
     auto clk = [] { return std::chrono::steady_clock::now(); };
@@ -814,8 +810,17 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     // phase 1 (device, in sample order): cuRAND streams, FMC masks, survivor
     // counts, coupling rescale; host copies of what the layout needs
     std::vector<std::vector<QuartetRec>> qsv(n);
-    std::vector<std::vector<double>> g4h(n), nrmv(n);
+    std::vector<std::vector<double>> g4h(n);
     std::vector<std::vector<uint8_t>> maskh(n);
+    // each sample's replica normals stay on the device until the normalisation
+    // kernel writes them, scaled, into the amplitude array
+    struct DevNormals {
+        std::vector<double*> p;
+        ~DevNormals() {
+            for (double* x : p) cudaFree(x);
+        }
+    } nrm_dev;
+    nrm_dev.p.assign(n, nullptr);
     for (int k = 0; k < n; k++) {
         SampleHost& h = s->hs[k];
         const int N = h.N, R = h.R;
@@ -833,11 +838,9 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         uint64_t master = h.cfg.seed;
         for (int r = 0; r < R; r++) keys[k][r] = splitmix64(master);
         // initial amplitudes: cuRAND normals per replica (spins.cu:75-82)
-        std::vector<double>& nrm = nrmv[k];
-        nrm.resize(2 * (size_t)N * R);
         {
-            double* d = nullptr;
-            rc = dalloc(&d, nrm.size());
+            double*& d = nrm_dev.p[k];
+            rc = dalloc(&d, 2 * (size_t)N * R);
             if (rc != PSPIN_OK) return bail(rc);
             // one generator, re-seeded with its offset reset for every
             // replica: the stream of a fresh generator with that seed
@@ -851,22 +854,16 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
                     cs = curandGenerateNormalDouble(c.g, d + 2 * (size_t)N * r, 2 * (size_t)N, 0.0, 1.0);
             }
             if (cs != CURAND_STATUS_SUCCESS) rc = fail(PSPIN_ERR_CURAND, "spin init cuRAND error %d", (int)cs);
-            if (rc == PSPIN_OK) {
-                cudaError_t e = cudaMemcpyAsync(nrm.data(), d, nrm.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st);
-                if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
-                if (e != cudaSuccess) rc = fail(PSPIN_ERR_CUDA, "spin init copy: %s", cudaGetErrorString(e));
-            }
-            cudaFree(d);
             if (rc != PSPIN_OK) return bail(rc);
         }
     }
     const auto t_p2 = clk();
-    // phase 2 (host, samples in parallel): normalisation, quartet lists,
-    // per-site sweep lists, FP64 quartet tables
+    // phase 2 (host, samples in parallel): quartet lists, per-site sweep
+    // lists, FP64 quartet tables
 #pragma omp parallel for schedule(dynamic, 1)
     for (int k = 0; k < n; k++) {
         SampleHost& h = s->hs[k];
-        const int N = h.N, R = h.R;
+        const int N = h.N;
         bool fc = false;
         if (variant == PSPIN_DENSE) {
             dense_quartets(N, g4h[k].data(), maskh[k].data(), qsv[k]);
@@ -879,15 +876,6 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
             std::vector<uint8_t>().swap(maskh[k]);
         }
         h.fc_tiles = fc ? 1 : 0;
-        targets[k].resize(R);
-        spins[k].resize((size_t)N * R);
-        for (int r = 0; r < R; r++) {
-            double* sp = nrmv[k].data() + 2 * (size_t)N * r;
-            targets[k][r] = normalize_host(sp, N, variant == PSPIN_SPARSE, s->opt.init_exact);
-            for (int i = 0; i < N; i++)
-                spins[k][(size_t)i * R + r] = make_float2((float)sp[2 * i], (float)sp[2 * i + 1]);
-        }
-        std::vector<double>().swap(nrmv[k]);
         if (!fc) build_site_lists(N, h.g2re.data(), h.h2_active, qsv[k], lists[k]);
         build_q64(qsv[k], q64[k]);
         std::vector<QuartetRec>().swap(qsv[k]);
@@ -937,8 +925,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     std::vector<Q64> qall(q_total);
     std::vector<uint32_t> nball(nb_total, 0u);
     std::vector<double> g2all(g2_total);
-    std::vector<float2> spall(s->spin_total);
-    std::vector<double> tall(s->R_tot), Eall(s->R_tot, 0.0);
+    std::vector<double> Eall(s->R_tot, 0.0);
     std::vector<uint64_t> kall(s->R_tot);
     {
         int64_t eoff = 0, coff = 0;
@@ -967,8 +954,6 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
                             if (a != b) set(a, b);
             }
             std::copy(s->hs[k].g2re.begin(), s->hs[k].g2re.end(), g2all.begin() + d.g2_off);
-            std::copy(spins[k].begin(), spins[k].end(), spall.begin() + d.spin_off);
-            std::copy(targets[k].begin(), targets[k].end(), tall.begin() + d.rep_off);
             std::copy(keys[k].begin(), keys[k].end(), kall.begin() + d.rep_off);
             lists[k] = SiteLists();
             q64[k].clear();
@@ -1033,8 +1018,6 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         for (int r = 0; r < s->hs[k].R; r++) ones[s->sd[k].rep_off + r] = 1.0 / s->hs[k].cfg.T;
     if ((rc = up(s->d_samples, s->sd.data(), n * sizeof(SampleDev))) ||
         (rc = up(s->d_units, s->units.data(), s->units.size() * sizeof(Unit))) ||
-        (rc = up(s->d_spins, spall.data(), spall.size() * sizeof(float2))) ||
-        (rc = up(s->d_target, tall.data(), tall.size() * sizeof(double))) ||
         (rc = up(s->d_key, kall.data(), kall.size() * sizeof(uint64_t))) ||
         (rc = up(s->d_entries, ent.data(), ent.size() * sizeof(int2))) ||
         (rc = up(s->d_site_chunks, site_chunks.data(), site_chunks.size() * sizeof(int))) ||
@@ -1056,6 +1039,15 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     if (s->opt.trace_replica >= 0 && s->opt.trace_capacity > 0) {
         if ((rc = dalloc(&s->d_trace, (size_t)s->opt.trace_capacity))) return bail(rc);
         cudaMemsetAsync(s->d_trace, 0, sizeof(pspin_move_record) * (size_t)s->opt.trace_capacity, s->st);
+    }
+    // replica amplitudes projected onto the constraint on the device, in the
+    // reference's way (spins.cu:27-111, spins_sparse.cu:28-80), as FP32 in the
+    // [site][replica] layout; each replica's constraint value as its target
+    for (int k = 0; k < n; k++) {
+        const SampleDev& d = s->sd[k];
+        cudaError_t e = dev_normalize_replicas(nrm_dev.p[k], d.N, d.R, variant == PSPIN_SPARSE, s->opt.init_exact,
+                                               s->d_spins + d.spin_off, s->d_target + d.rep_off, s->st);
+        if (e != cudaSuccess) return bail(fail(PSPIN_ERR_CUDA, "spin normalisation: %s", cudaGetErrorString(e)));
     }
     // initial energies (the chain's form, FP64, from the FP32 amplitudes)
     if ((rc = run_energy(s, nullptr, nullptr, true, false))) return bail(rc);

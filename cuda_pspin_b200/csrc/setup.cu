@@ -9,6 +9,7 @@
 // it p = C(j,2)+i.  Blocks in (l,k) lexicographic order are blocks in q
 // order, which is what the sparse selection needs (mc_sparse.cu:491-500).
 #include "internal.h"
+#include <algorithm>
 #include <cstdint>
 
 namespace pspin {
@@ -125,6 +126,108 @@ __global__ void roundtrip_kernel(int N, int64_t nq, unsigned long long* fails) {
 }
 
 // ---------------------------------------------------------------- hosts
+
+// ---- g2 (disorder.cu:45-80, 130-143, 191-197; mc.cu:469-477, 436-502) ------
+// g2[i][j] <- Re of normal (min(i,j), max(i,j)) (imaginary parts dropped,
+// lower triangle copied from the upper one, diagonal kept); with uniform
+// FMC, i != j with |w_i - w_j| > gamma set to 0 (both halves); *count <- the
+// non-zero entries with i <= j.
+__global__ void g2_build_kernel(const double* __restrict__ normals, int N, const double* __restrict__ omega,
+                                double gamma, double* __restrict__ g2, unsigned long long* __restrict__ count) {
+    const long long total = (long long)N * N;
+    for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+         id += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(id / N), j = (int)(id % N);
+        const long long src = (i > j) ? (long long)j * N + i : (long long)i * N + j;
+        double v = normals[2 * src];
+        if (omega != nullptr && i != j && fabs(omega[i] - omega[j]) > gamma) v = 0.0;
+        g2[id] = v;
+        if (i <= j && v != 0.0) atomicAdd(count, 1ull);
+    }
+}
+
+// g2 <- g2 sigma, then + mean on the non-zero entries
+__global__ void g2_scale_kernel(double* __restrict__ g2, long long n, double sigma, double mean, int shift) {
+    for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < n;
+         id += (long long)gridDim.x * blockDim.x) {
+        double v = g2[id] * sigma;
+        if (shift && v != 0.0) v += mean;
+        g2[id] = v;
+    }
+}
+
+// ---- replica initialisation (spins.cu:27-69, 84-111; spins_sparse.cu:28-80)
+// One CTA per replica, blockDim as the reference launches its normalisation
+// (sphere: N up to 1024, cube: N rounded up to a multiple of 32, >= 32, up to
+// 1024), the same shared-memory tree and expressions, so the scale is the
+// reference's -- including its truncation for N not a power of two (the
+// tree starts at blockDim/2) and, for the cube beyond 1024 sites, scaling
+// only the first 1024.  exact = 1 (or a sphere beyond 1024 sites, which the
+// reference sums on the host) sums every site in order instead.  The
+// amplitudes are written as FP32 into the sample's [site][replica] layout,
+// target[r] <- the constraint value of the scaled amplitudes (FP64, in site
+// order).
+__global__ void normalize_replicas_kernel(const double* __restrict__ nrm, int N, int R, int cube, int exact,
+                                          float2* __restrict__ spins, double* __restrict__ target) {
+    extern __shared__ double sdata[];
+    const int r = blockIdx.x, tid = threadIdx.x;
+    const double* a = nrm + (size_t)r * 2 * N;
+    __shared__ double scale_s;
+    const bool seq = exact || (!cube && N > 1024);
+    if (seq) {
+        if (tid == 0) {
+            double sum = 0.0;
+            for (int i = 0; i < N; i++) {
+                const double r2 = __dadd_rn(__dmul_rn(a[2 * i], a[2 * i]), __dmul_rn(a[2 * i + 1], a[2 * i + 1]));
+                sum = __dadd_rn(sum, cube ? __dmul_rn(r2, r2) : r2);
+            }
+            scale_s = cube ? pow((double)N / sum, 0.25) : sqrt((double)N / sum);
+        }
+    } else {
+        double local = 0.0;
+        if (tid < N) {
+            const double re = a[2 * tid], im = a[2 * tid + 1];
+            if (cube) {
+                const double r2 = re * re + im * im;
+                local = r2 * r2;
+            } else {
+                local = re * re + im * im;
+            }
+        }
+        sdata[tid] = local;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (tid < s) sdata[tid] += sdata[tid + s];
+            __syncthreads();
+        }
+        if (tid == 0) scale_s = cube ? pow((double)N / sdata[0], 0.25) : sqrt((double)N / sdata[0]);
+    }
+    __syncthreads();
+    const double scale = scale_s;
+    const int lim = (seq || !cube) ? N : min(N, (int)blockDim.x);
+    for (int i = tid; i < N; i += blockDim.x) {
+        double re = a[2 * i], im = a[2 * i + 1];
+        if (i < lim) {
+            re *= scale;
+            im *= scale;
+        }
+        spins[(size_t)i * R + r] = make_float2((float)re, (float)im);
+    }
+    if (tid == 0) {
+        double t = 0.0;
+        for (int i = 0; i < N; i++) {
+            double re = a[2 * i], im = a[2 * i + 1];
+            if (i < lim) {
+                re = __dmul_rn(re, scale);
+                im = __dmul_rn(im, scale);
+            }
+            const double r2 = __dadd_rn(__dmul_rn(re, re), __dmul_rn(im, im));
+            t = __dadd_rn(t, cube ? __dmul_rn(r2, r2) : r2);
+        }
+        target[r] = t;
+    }
+}
+
 cudaError_t dev_fmc_mask(uint8_t* mask, const double* omega, int N, double gamma, cudaStream_t st) {
     fmc_mask_kernel<<<dim3(N, N), 256, N * sizeof(double), st>>>(mask, omega, N, gamma);
     return cudaGetLastError();
@@ -167,6 +270,34 @@ cudaError_t dev_roundtrip(int N, int64_t nq, unsigned long long* fails, cudaStre
     if (e != cudaSuccess) return e;
     if (nq <= 0) return cudaSuccess;
     roundtrip_kernel<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(N, nq, fails);
+    return cudaGetLastError();
+}
+
+
+cudaError_t dev_g2_build(const double* normals, int N, const double* omega, double gamma, double* g2,
+                         unsigned long long* count, cudaStream_t st) {
+    const long long total = (long long)N * N;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 8);
+    g2_build_kernel<<<blocks, 256, 0, st>>>(normals, N, omega, gamma, g2, count);
+    return cudaGetLastError();
+}
+
+cudaError_t dev_g2_scale(double* g2, long long n, double sigma, double mean, int shift, cudaStream_t st) {
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 8);
+    if (n > 0) g2_scale_kernel<<<blocks, 256, 0, st>>>(g2, n, sigma, mean, shift);
+    return cudaGetLastError();
+}
+
+// the reference's block size for each normalisation (spins.cu:89, spins_sparse.cu:76)
+cudaError_t dev_normalize_replicas(const double* nrm, int N, int R, int cube, int exact, float2* spins,
+                                   double* target, cudaStream_t st) {
+    int bd = (N < 1024) ? N : 1024;
+    if (cube) {
+        bd = (N < 1024) ? (N + 31) / 32 * 32 : 1024;
+        if (bd < 32) bd = 32;
+    }
+    if (R > 0)
+        normalize_replicas_kernel<<<R, bd, bd * sizeof(double), st>>>(nrm, N, R, cube, exact, spins, target);
     return cudaGetLastError();
 }
 
