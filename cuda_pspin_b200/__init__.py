@@ -421,10 +421,10 @@ class Engine:
 
     def learn_params(self, set_to=None) -> np.ndarray:
         out = np.empty(MLP_PARAMS, np.float32)
-        src = None if set_to is None else _ptr(np.ascontiguousarray(set_to, np.float32))
-        _check(self._lib.pspin_learn_params(self._h, _ptr(out), src))
-        if set_to is not None:
-            out = np.ascontiguousarray(set_to, np.float32).copy()
+        w = None if set_to is None else np.ascontiguousarray(set_to, np.float32)   # alive across the call
+        _check(self._lib.pspin_learn_params(self._h, _ptr(out), None if w is None else _ptr(w)))
+        if w is not None:
+            out = w.copy()
         return out
 
     def learn_train(self, steps: int, batch: int = 4096, lr: float = 1e-3) -> float:

@@ -110,7 +110,8 @@ def omega(N: int, fmc_mode: int, seed: int) -> np.ndarray:
 
 def fmc_mask(N: int, w: np.ndarray, gamma: float) -> np.ndarray:
     m = np.zeros(n_quartets(N), np.uint8)
-    lib().orc_fmc_g4_mask(P(m), N, P(np.ascontiguousarray(w, np.float64)), gamma)
+    wc = np.ascontiguousarray(w, np.float64)
+    lib().orc_fmc_g4_mask(P(m), N, P(wc), gamma)
     return m
 
 
@@ -278,8 +279,9 @@ def check_trace(ref, spins0: np.ndarray, trace: np.ndarray, tol: float = 1e-5, r
             rels.append(err / abs(d64))
         if g2d is not None:
             # hamiltonian.cu form, computed on its own (g2 over i <= j, hamiltonian.cu:30-38)
-            hs = [lib().orc_energy_h2_with_diag(len(s), P(g2c), P(np.ascontiguousarray(
-                np.stack([v.real, v.imag], -1).ravel()))) for v in (s, new)]
+            # the interleaved copies must outlive the calls that read them
+            flat = [np.ascontiguousarray(np.stack([v.real, v.imag], -1).ravel()) for v in (s, new)]
+            hs = [lib().orc_energy_h2_with_diag(len(s), P(g2c), P(f)) for f in flat]
             d_ham = (hs[1] + e4n) - (hs[0] + e4o)
             dd = sum(-g2d[k] * (abs(new[k]) ** 2 - abs(s[k]) ** 2) for k in (i0, j0))   # its diagonal part
             diag_max = max(diag_max, abs(d_ham - d64) / scale if scale > 0 else abs(d_ham - d64))

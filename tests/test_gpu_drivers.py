@@ -263,7 +263,8 @@ def test_gpu_deeper_analysis_matches_analysis_pt(tmp_path, variant):
     if sparse:
         flags += ["-fmc", "1", "-gamma", "1"]
     run([os.path.join(BIN, "pspin_pt_sparse" if sparse else "pspin_pt"), *flags], tmp_path)
-    run([os.path.join(REF, "analysis_pt"), "-N", N, "-NT", "4", "-nrep", "3", "--log-temp", "--deeper"], tmp_path)
+    run([os.path.join(REF, "analysis_pt"), "-N", N, "-NT", "4", "-nrep", "3", "--log-temp", "--deeper",
+         *(["--sparse"] if sparse else [])], tmp_path)
     p = subprocess.run([sys.executable, "-m", "cuda_pspin_b200.analysis", "-N", N, "-NT", "4", "-nrep", "3",
                         "--deeper", "--out", str(tmp_path / "gpu")], cwd=tmp_path, capture_output=True, text=True,
                        timeout=600, env={**os.environ, "PYTHONPATH": ROOT})

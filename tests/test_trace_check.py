@@ -37,9 +37,9 @@ def _trace(ref, s0, n_moves, seed, plant=None):
     return out
 
 
-@pytest.mark.parametrize("fmc", [0, 2])
-def test_check_trace_reports(orc, fmc):
-    ref = orc.DenseInit(orc.cfg(N=10, nrep=1, fmc_mode=fmc, seed=5, gamma=0.3 if fmc else 0.0))
+@pytest.mark.parametrize("N,fmc", [(10, 0), (10, 2), (64, 0)])
+def test_check_trace_reports(orc, N, fmc):
+    ref = orc.DenseInit(orc.cfg(N=N, nrep=1, fmc_mode=fmc, seed=5, gamma=0.3 if fmc else 0.0))
     s0 = ref.spins_c()[0].astype(np.complex64).astype(np.complex128)
     tr = _trace(ref, s0, 40, 1)
     rep = {}
