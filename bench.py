@@ -147,7 +147,8 @@ def run_engine(args, rank, world, device, dist):
     t_setup = time.perf_counter()
     shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else None
     opts = ps.make_options(resync_every=1024, warps_per_unit=shape[0] if shape else 0,
-                           cluster_size=(shape[1] if shape[1] > 0 else -1) if shape else 0)
+                           cluster_size=(shape[1] if shape[1] > 0 else -1) if shape else 0,
+                           replicas_per_lane=shape[2] if shape and len(shape) > 2 else 0)
     eng = ps.Engine(cfgs, ps.PSPIN_DENSE, opts)
     t_setup = time.perf_counter() - t_setup
     eng.pt_init(NT, NREP_T, beta, 1)
@@ -166,9 +167,10 @@ def run_engine(args, rank, world, device, dist):
     # block shape by the engine's autotuner (state restored after its trials),
     # then one more step so the PT graph is captured with that shape
     if shape:
-        tuned_w, tuned_c = shape
+        tuned_w, tuned_c = shape[:2]
+        tuned_k = shape[2] if len(shape) > 2 else 1
     else:
-        tuned_w, tuned_c, tuned_ms = eng.autotune(2)
+        tuned_w, tuned_c, tuned_k, tuned_ms = eng.autotune_lanes(2)
     eng.pt_run(sps)
     eng.get_profile()                  # zero the launch counters
     ext = torch.cuda.ExternalStream(eng.stream_ptr(), device=device)
@@ -213,8 +215,11 @@ def run_engine(args, rank, world, device, dist):
     if os.path.exists(tf):
         try:
             rec = json.load(open(tf))
-            # the capture of the kernel this launch ran: cluster split or one CTA
-            if tuned_c == 1 and "one_cta_kernel" in rec:
+            # the capture of the kernel this launch ran: cluster split, one CTA,
+            # or K replicas per lane
+            if tuned_k > 1:
+                rec = rec.get(f"replicas_per_lane_{tuned_k}", {})
+            elif tuned_c == 1 and "one_cta_kernel" in rec:
                 rec = rec["one_cta_kernel"]
             traffic = None if tuned_c == 0 else rec.get("bytes_per_launch")
         except Exception:
@@ -306,7 +311,8 @@ def run_engine(args, rank, world, device, dist):
                    "l2": f"inputs exceed L2: {entries * 8 / 1e9:.2f} GB of site lists per GPU (no flush)",
                    "parallelism": f"samples sharded, {world} GPU(s), no collective",
                    "block_shape": {"warps_per_cta": tuned_w, "ctas_per_replica_block": tuned_c,
-                                   "chosen_by": "--shape" if shape else "pspin_autotune (2 sweeps per shape)"},
+                                   "replicas_per_lane": tuned_k,
+                                   "chosen_by": "--shape" if shape else "pspin_autotune_lanes (2 sweeps per shape)"},
                    "launch": "sweep + exchange per PT step, replayed as CUDA graphs of 32 steps",
                    "setup_s": t_setup},
         "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "resync": resync,
@@ -386,8 +392,8 @@ def main():
     ap.add_argument("--sweeps-per-step", type=int, default=16)
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--shape", default="", help="W,C: warps per CTA, CTAs per replica block (skips the autotuner; "
-                                                "for profiling a fixed kernel shape)")
+    ap.add_argument("--shape", default="", help="W,C[,K]: warps per CTA, CTAs per replica block, replicas per "
+                                                "lane (skips the autotuner; for profiling a fixed kernel shape)")
     ap.add_argument("--workload", default="batched", choices=["batched", "learned"])
     ap.add_argument("--equilibrate", type=int, default=1 << 15,
                     help="learned workload: plain PT sweeps between training and measuring")

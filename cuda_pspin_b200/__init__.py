@@ -66,7 +66,7 @@ class Options(ctypes.Structure):
                 ("quiet", ctypes.c_int), ("generic_lists", ctypes.c_int), ("graph_steps", ctypes.c_int),
                 ("resync_method", ctypes.c_int), ("cluster_size", ctypes.c_int),
                 ("wait_limit_clocks", ctypes.c_int), ("test_stall_move", ctypes.c_int),
-                ("disorder_stream", ctypes.c_int)]
+                ("disorder_stream", ctypes.c_int), ("replicas_per_lane", ctypes.c_int)]
 
 
 class Info(ctypes.Structure):
@@ -143,6 +143,7 @@ def load_library() -> ctypes.CDLL:
         "pspin_set_proposal": (ctypes.c_int, [vp, ctypes.c_int]),
         "pspin_observe_init": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
         "pspin_autotune": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp]),
+        "pspin_autotune_lanes": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp, vp]),
         "pspin_resync_drift": (ctypes.c_int, [vp, vp]),
         "pspin_checkpoint_save": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "pspin_pt_shape": (ctypes.c_int, [vp, vp, vp, vp]),
@@ -206,9 +207,10 @@ def make_options(init_exact: bool = False, resync_every: int = 0, warps_per_unit
                  trace: tuple[int, int, int] | None = None, quiet: bool = True,
                  generic_lists: bool = False, graph_steps: int = 0, resync_method: int = 0,
                  cluster_size: int = 0, wait_limit_clocks: int = 0, test_stall_move: int = 0,
-                 disorder_stream: bool = False) -> Options:
+                 disorder_stream: bool = False, replicas_per_lane: int = 0) -> Options:
     o = Options()
     o.disorder_stream = int(disorder_stream)
+    o.replicas_per_lane = int(replicas_per_lane)
     o.cluster_size = int(cluster_size)
     o.wait_limit_clocks = int(wait_limit_clocks)
     o.test_stall_move = int(test_stall_move)
@@ -386,6 +388,15 @@ class Engine:
         ms = np.zeros((6, 4), np.float32)
         _check(self._lib.pspin_autotune(self._h, int(sweeps), ctypes.byref(w), ctypes.byref(c), _ptr(ms)))
         return w.value, c.value, ms
+
+    def autotune_lanes(self, sweeps: int = 8):
+        """Plain sweep: (warps, cluster, replicas per lane, ms per sweep
+        [replicas per lane 1, 2, 3][resident, cluster 1, 2, 4, 8, 16][warps 1, 2, 4, 8])."""
+        w, c, k = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        ms = np.zeros((3, 6, 4), np.float32)
+        _check(self._lib.pspin_autotune_lanes(self._h, int(sweeps), ctypes.byref(w), ctypes.byref(c),
+                                              ctypes.byref(k), _ptr(ms)))
+        return w.value, c.value, k.value, ms
 
     def observe_init(self, temp_index: int, capacity: int) -> None:
         _check(self._lib.pspin_observe_init(self._h, int(temp_index), int(capacity)))

@@ -24,7 +24,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "noalloc.cu", "sweep_cluster.cu", "sweep_resident.cu", "analysis.cu", "tcfield.cu", "learned.cu", "cube.cu", "layout.cpp"]
+LIB_SOURCES = ["abi.cu", "sweep.cu", "pt.cu", "setup.cu", "noalloc.cu", "sweep_cluster.cu", "sweep_multi.cu", "sweep_resident.cu", "analysis.cu", "tcfield.cu", "learned.cu", "cube.cu", "layout.cpp"]
 
 
 def cutlass_dir() -> str:

@@ -153,12 +153,15 @@ struct pspin_state {
     int R_tot = 0, max_N = 0, warps = 8, cluster = 1;   // cluster 0: list-resident one-warp kernel
     int64_t max_site_entries = 0;
     int warps2 = 8, cluster2 = 1;       // block shape of the two-pass (learned / fields) sweep
+    int rpl = 1;                        // replicas per lane of the plain CTA / cluster sweep
+    std::vector<Unit> units_k[2];       // blocks of 64 and 96 replicas (rpl 2, 3)
     int64_t spin_total = 0;
     cudaStream_t st = nullptr;
     int device = 0;
 
     SampleDev* d_samples = nullptr;
     Unit* d_units = nullptr;
+    Unit* d_units_k[2] = {nullptr, nullptr};
     float2* d_spins = nullptr;
     double *d_E = nullptr, *d_beta = nullptr, *d_target = nullptr, *d_drift = nullptr, *d_e2 = nullptr,
            *d_e4 = nullptr;
@@ -243,7 +246,8 @@ static void free_state(pspin_state* s) {
                     s->d_beta_sched, s->d_perm, s->d_drand, s->d_ex_acc, s->d_ex_prop, s->d_trace,
                     s->d_tc_w, s->d_tc_x, s->d_tc_f, s->d_tc_ws, s->d_tc_h, s->d_f64_h, s->d_tc_e,
                     s->d_w32, s->d_adam_m, s->d_adam_v, s->d_grad, s->d_wbf, s->d_records, s->d_rec_count,
-                    s->d_save, s->d_loss, s->d_idx, s->d_obs_E, s->d_obs_q, s->d_pair_chunks, s->d_nbmask};
+                    s->d_save, s->d_loss, s->d_idx, s->d_obs_E, s->d_obs_q, s->d_pair_chunks, s->d_nbmask,
+                    s->d_units_k[0], s->d_units_k[1]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& e : s->ev_pool) {
@@ -966,9 +970,17 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     for (int k = 0; k < n; k++)
         for (int rb = 0; rb < s->hs[k].R; rb += kRepBlock)
             s->units.push_back(Unit{k, rb, std::min(kRepBlock, s->hs[k].R - rb), 0});
-    std::stable_sort(s->units.begin(), s->units.end(), [&](const Unit& a, const Unit& b) {
-        return s->hs[a.sample].site_entries > s->hs[b.sample].site_entries;
-    });
+    for (int K = 2; K <= 3; K++)
+        for (int k = 0; k < n; k++)
+            for (int rb = 0; rb < s->hs[k].R; rb += K * kRepBlock)
+                s->units_k[K - 2].push_back(Unit{k, rb, std::min(K * kRepBlock, s->hs[k].R - rb), 0});
+    for (std::vector<Unit>* u : {&s->units, &s->units_k[0], &s->units_k[1]})
+        std::stable_sort(u->begin(), u->end(), [&](const Unit& a, const Unit& b) {
+            return s->hs[a.sample].site_entries > s->hs[b.sample].site_entries;
+        });
+    if (s->opt.replicas_per_lane < 0 || s->opt.replicas_per_lane > 3)
+        return bail(fail(PSPIN_ERR_ARG, "replicas_per_lane must be 0, 1, 2 or 3"));
+    s->rpl = std::max(1, s->opt.replicas_per_lane);
     s->warps = choose_warps(s);
     if (s->warps < 0) return bail(fail(PSPIN_ERR_ARG, "warps_per_unit must be 1, 2, 4 or 8"));
     if (s->opt.wait_limit_clocks < 0 || s->opt.test_stall_move < 0)
@@ -993,6 +1005,9 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
     }
     if (sweep_smem_bytes(s->max_N, s->warps) > 227 * 1024)
         return bail(fail(PSPIN_ERR_ARG, "N=%d needs more shared memory than a CTA has", s->max_N));
+    if (s->rpl > 1 && s->cluster >= 1 && multi_smem_bytes_host(s->max_N, s->warps, s->cluster, s->rpl) > 227 * 1024)
+        return bail(fail(PSPIN_ERR_ARG, "N=%d with %d replicas per lane needs more shared memory than a CTA has",
+                         s->max_N, s->rpl));
 
     if ((rc = dalloc(&s->d_samples, n)) || (rc = dalloc(&s->d_units, s->units.size())) ||
         (rc = dalloc(&s->d_spins, (size_t)s->spin_total)) || (rc = dalloc(&s->d_E, s->R_tot)) ||
@@ -1005,7 +1020,8 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         (rc = dalloc(&s->d_q64, (size_t)std::max<int64_t>(q_total, 1))) ||
         (rc = dalloc(&s->d_g2, (size_t)g2_total)) || (rc = dalloc(&s->d_sweep_counter, 1)) ||
         (rc = dalloc(&s->d_nbmask, (size_t)std::max<int64_t>(nb_total, 1))) ||
-        (rc = dalloc(&s->d_status, 1)))
+        (rc = dalloc(&s->d_status, 1)) || (rc = dalloc(&s->d_units_k[0], s->units_k[0].size())) ||
+        (rc = dalloc(&s->d_units_k[1], s->units_k[1].size())))
         return bail(rc);
     auto up = [&](void* dst, const void* src, size_t bytes) -> int {
         if (!bytes) return PSPIN_OK;
@@ -1018,6 +1034,8 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         for (int r = 0; r < s->hs[k].R; r++) ones[s->sd[k].rep_off + r] = 1.0 / s->hs[k].cfg.T;
     if ((rc = up(s->d_samples, s->sd.data(), n * sizeof(SampleDev))) ||
         (rc = up(s->d_units, s->units.data(), s->units.size() * sizeof(Unit))) ||
+        (rc = up(s->d_units_k[0], s->units_k[0].data(), s->units_k[0].size() * sizeof(Unit))) ||
+        (rc = up(s->d_units_k[1], s->units_k[1].data(), s->units_k[1].size() * sizeof(Unit))) ||
         (rc = up(s->d_key, kall.data(), kall.size() * sizeof(uint64_t))) ||
         (rc = up(s->d_entries, ent.data(), ent.size() * sizeof(int2))) ||
         (rc = up(s->d_site_chunks, site_chunks.data(), site_chunks.size() * sizeof(int))) ||
@@ -1111,6 +1129,10 @@ static int enqueue_step(pspin_state* s, int nsweeps, bool exchange, cudaEvent_t 
     p.cluster = s->proposal == PSPIN_PROPOSAL_PLAIN ? s->cluster : s->cluster2;
     if (s->proposal == PSPIN_PROPOSAL_PLAIN && s->cluster == 0) {
         CK(launch_sweep_resident(p, (int)s->units.size(), s->variant, s->max_N, s->max_site_entries, s->st));
+    } else if (s->proposal == PSPIN_PROPOSAL_PLAIN && s->rpl > 1) {
+        const std::vector<Unit>& u = s->units_k[s->rpl - 2];
+        p.units = s->d_units_k[s->rpl - 2];
+        CK(launch_sweep_multi(p, (int)u.size(), s->variant, s->max_N, s->rpl, s->st, nullptr));
     } else if (s->proposal == PSPIN_PROPOSAL_PLAIN && s->cluster > 1) {
         CK(launch_sweep_cluster(p, (int)s->units.size(), s->variant, s->max_N, s->st, nullptr));
     } else if (s->proposal == PSPIN_PROPOSAL_PLAIN) {
@@ -1284,11 +1306,24 @@ static int run_sweeps(pspin_state* s, int nsweeps, bool pt) {
 
 // Whether `cluster` CTAs of `warps` warps can hold one replica block (shared
 // memory, co-residency of the cluster); the plain kernel for cluster 1.
-static bool shape_fits(pspin_state* s, int warps, int cluster) {
+static bool shape_fits(pspin_state* s, int warps, int cluster, int K = 1) {
     if (cluster == 0)
-        return s->proposal == PSPIN_PROPOSAL_PLAIN &&
+        return K == 1 && s->proposal == PSPIN_PROPOSAL_PLAIN &&
                resident_smem_bytes_host(s->max_N, s->max_site_entries, warps) <= 227 * 1024;
     if (cluster * warps > kSplit) return false;
+    if (K > 1) {
+        if (s->proposal != PSPIN_PROPOSAL_PLAIN) return false;
+        if (multi_smem_bytes_host(s->max_N, warps, cluster, K) > 227 * 1024) return false;
+        SweepParams p{};
+        p.warps = warps;
+        p.cluster = cluster;
+        int n = 0;
+        if (launch_sweep_multi(p, (int)s->units_k[K - 2].size(), s->variant, s->max_N, K, s->st, &n) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return n > 0;
+    }
     if (s->proposal != PSPIN_PROPOSAL_PLAIN) {
         if (learned_smem_bytes_host(s->max_N, warps, cluster) > 227 * 1024) return false;
         if (cluster == 1) return true;
@@ -1321,7 +1356,8 @@ static bool shape_fits(pspin_state* s, int warps, int cluster) {
 // keeps the fastest.  The state (amplitudes, energies, counters, sweep index)
 // is restored after every trial, so the chain continues as if the trials had
 // not run.
-extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int* chosen_cluster, float* ms_out) {
+static int autotune(pspin_state* s, int sweeps, int k_lo, int k_hi, int* chosen_warps, int* chosen_cluster,
+                    int* chosen_k, float* ms_out) {
     if (!s || sweeps < 1) return fail(PSPIN_ERR_ARG, "bad arguments");
     float2* b_spins = nullptr;
     double* b_E = nullptr;
@@ -1347,7 +1383,7 @@ extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int
     const bool plain = s->proposal == PSPIN_PROPOSAL_PLAIN;
     int& W = plain ? s->warps : s->warps2;   // the current proposal's kernel is tuned
     int& Cl = plain ? s->cluster : s->cluster2;
-    const int w0 = W, c0 = Cl;
+    const int w0 = W, c0 = Cl, k0 = s->rpl;
     const float prob0 = s->rec_prob;
     s->rec_prob = 0.f;                       // trials record no training moves
     cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -1355,15 +1391,17 @@ extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int
     if (e == cudaSuccess) e = copy_all(true);
     if (e == cudaSuccess) e = cudaEventCreate(&t0);
     if (e == cudaSuccess) e = cudaEventCreate(&t1);
-    int best_w = w0, best_c = c0;
+    int best_w = w0, best_c = c0, best_k = k0;
     float best_ms = 0.f;
     const int cw[4] = {1, 2, 4, 8}, cc[6] = {0, 1, 2, 4, 8, 16};
+    for (int K = k_lo; K <= k_hi; K++)
     for (int ci = 0; ci < 6; ci++)
         for (int wi = 0; wi < 4; wi++) {
             float ms = -1.f;
-            if (e == cudaSuccess && rc == PSPIN_OK && shape_fits(s, cw[wi], cc[ci])) {
+            if (e == cudaSuccess && rc == PSPIN_OK && shape_fits(s, cw[wi], cc[ci], K)) {
                 W = cw[wi];
                 Cl = cc[ci];
+                if (plain) s->rpl = K;
                 rc = enqueue_step(s, 1, false, nullptr, nullptr);          // warm-up sweep
                 if (rc == PSPIN_OK) e = cudaEventRecord(t0, s->st);
                 for (int k = 0; k < sweeps && rc == PSPIN_OK && e == cudaSuccess; k++)
@@ -1373,11 +1411,16 @@ extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int
                 if (rc == PSPIN_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
                 if (rc == PSPIN_OK && e == cudaSuccess) {
                     ms /= sweeps;
-                    if (best_ms <= 0.f || ms < best_ms) { best_ms = ms; best_w = cw[wi]; best_c = cc[ci]; }
+                    if (best_ms <= 0.f || ms < best_ms) {
+                        best_ms = ms;
+                        best_w = cw[wi];
+                        best_c = cc[ci];
+                        best_k = K;
+                    }
                 }
                 if (e == cudaSuccess) e = copy_all(false);
             }
-            if (ms_out) ms_out[ci * 4 + wi] = ms;
+            if (ms_out) ms_out[((K - k_lo) * 6 + ci) * 4 + wi] = ms;
         }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
     int status = 0;
@@ -1389,13 +1432,29 @@ extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int
     const bool good = rc == PSPIN_OK && e == cudaSuccess;
     W = good ? best_w : w0;
     Cl = good ? best_c : c0;
+    if (plain) s->rpl = good ? best_k : k0;
     drop_graph(s);
     if (rc != PSPIN_OK) return rc;
     if (e != cudaSuccess) return fail(PSPIN_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
     if (status) return timeout_error(status);
     if (chosen_warps) *chosen_warps = W;
     if (chosen_cluster) *chosen_cluster = Cl;
+    if (chosen_k) *chosen_k = plain ? s->rpl : 1;
     return PSPIN_OK;
+}
+
+extern "C" int pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int* chosen_cluster, float* ms_out) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    const int K = s->proposal == PSPIN_PROPOSAL_PLAIN ? s->rpl : 1;
+    return autotune(s, sweeps, K, K, chosen_warps, chosen_cluster, nullptr, ms_out);
+}
+
+extern "C" int pspin_autotune_lanes(pspin_state* s, int sweeps, int* chosen_warps, int* chosen_cluster,
+                                    int* chosen_replicas_per_lane, float* ms_out) {
+    if (!s) return fail(PSPIN_ERR_ARG, "null handle");
+    if (s->proposal != PSPIN_PROPOSAL_PLAIN)
+        return fail(PSPIN_ERR_ARG, "pspin_autotune_lanes tunes the plain sweep (use pspin_autotune)");
+    return autotune(s, sweeps, 1, 3, chosen_warps, chosen_cluster, chosen_replicas_per_lane, ms_out);
 }
 
 extern "C" int pspin_sweep(pspin_state* s, int nsweeps) { return run_sweeps(s, nsweeps, false); }

@@ -133,6 +133,11 @@ cudaError_t launch_sweep(const SweepParams& p, int n_units, int variant, int max
 cudaError_t launch_sweep_cluster(const SweepParams& p, int n_units, int variant, int max_N, cudaStream_t st,
                                  int* max_clusters);
 size_t cluster_smem_bytes_host(int N, int warps, int C);
+// the CTA / cluster kernel with K = 2 or 3 replicas per lane (units of up to
+// 32K replicas of one sample); cluster 1 launches no cluster
+cudaError_t launch_sweep_multi(const SweepParams& p, int n_units, int variant, int max_N, int K, cudaStream_t st,
+                               int* max_clusters);
+size_t multi_smem_bytes_host(int N, int warps, int C, int K);
 // the list-resident kernel; warps > 1 runs batches of consecutive moves that
 // commute (no site of one in the other's quartet neighbourhood) on separate
 // warps, with the neighbour masks `nbmask`

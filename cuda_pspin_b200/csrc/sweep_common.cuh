@@ -277,6 +277,95 @@ __device__ __forceinline__ void accumulate_tiles(const int2* __restrict__ R2, in
     }
 }
 
+// ---------------------------------------------------------------- K replicas per lane
+// The same accumulations for a block of 32K replicas stored [site][K][32]
+// (replica k*32 + lane of the block at sp[(site*K + k)*32 + lane]): each
+// staged coupling is read once and used for the lane's K replicas.  The
+// summation order per replica is that of accumulate_chunk / accumulate_tiles.
+template <int K>
+__device__ __forceinline__ void accumulate_chunk_k(const int2* __restrict__ R, int n,
+                                                   const float2* __restrict__ sp, int lane,
+                                                   float (&hx)[K], float (&hy)[K]) {
+    int e = 0;
+    while (e < n) {
+        const int2 h = R[e];
+        const int len = h.x;
+        const int p = h.y >> 16, o1 = h.y & 0xFFFF;
+        float yx[K], yy[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) yx[k] = yy[k] = 0.f;
+        const int2* __restrict__ d = R + e + 1;
+#pragma unroll 4
+        for (int t = 0; t < len; t++) {
+            const int2 v = d[t];
+            const float g = __int_as_float(v.x);
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const float2 a = sp[(v.y * K + k) * kRepBlock + lane];
+                yx[k] = fmaf(g, a.x, yx[k]);
+                yy[k] = fmaf(-g, a.y, yy[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const float2 ap = sp[(p * K + k) * kRepBlock + lane];
+            const float2 ao = sp[(o1 * K + k) * kRepBlock + lane];
+            const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
+            const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
+            hx[k] = fmaf(px, yx[k], fmaf(-py, yy[k], hx[k]));
+            hy[k] = fmaf(px, yy[k], fmaf(py, yx[k], hy[k]));
+        }
+        e += len + 1;
+    }
+}
+
+template <int K, int kUnroll>
+__device__ __forceinline__ void accumulate_tiles_k(const int2* __restrict__ R2, int n,
+                                                   const float2* __restrict__ sp, int lane,
+                                                   float (&hx)[K], float (&hy)[K]) {
+    const int4* __restrict__ R = reinterpret_cast<const int4*>(R2);
+    const int n16 = n >> 1;
+    int e = 0;
+    while (e < n16) {
+        const int4 hd = R[e];
+        const int outer = hd.x & 0xFFFF, lo = hd.x >> 16, hi = hd.y;
+        float y[K][8];
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+            for (int q = 0; q < 8; q++) y[k][q] = 0.f;
+        const float4* __restrict__ C = reinterpret_cast<const float4*>(R + e + 1);
+        const float2* __restrict__ A = sp + (size_t)lo * K * kRepBlock + lane;
+        const int len = hi - lo;
+#pragma unroll kUnroll
+        for (int t = 0; t < len; t++) {
+            const float4 c = C[t];
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const float2 a = A[(t * K + k) * kRepBlock];
+                y[k][0] = fmaf(c.x, a.x, y[k][0]); y[k][1] = fmaf(-c.x, a.y, y[k][1]);
+                y[k][2] = fmaf(c.y, a.x, y[k][2]); y[k][3] = fmaf(-c.y, a.y, y[k][3]);
+                y[k][4] = fmaf(c.z, a.x, y[k][4]); y[k][5] = fmaf(-c.z, a.y, y[k][5]);
+                y[k][6] = fmaf(c.w, a.x, y[k][6]); y[k][7] = fmaf(-c.w, a.y, y[k][7]);
+            }
+        }
+        const int pk[4] = {hd.z & 0xFFFF, hd.z >> 16, hd.w & 0xFFFF, hd.w >> 16};
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const float2 ao = sp[(outer * K + k) * kRepBlock + lane];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const float2 ap = sp[(pk[q] * K + k) * kRepBlock + lane];
+                const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
+                const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
+                hx[k] = fmaf(px, y[k][2 * q], fmaf(-py, y[k][2 * q + 1], hx[k]));
+                hy[k] = fmaf(px, y[k][2 * q + 1], fmaf(py, y[k][2 * q], hy[k]));
+            }
+        }
+        e += 1 + len;
+    }
+}
+
 // ---------------------------------------------------------------- clusters
 // Partial fields of the CTAs of a thread-block cluster meet in every CTA's
 // exchange buffer (distributed shared memory).

@@ -117,6 +117,14 @@ typedef struct pspin_options {
                             values, with no C(N,4)-sized memory.  The FMC
                             survivors and the quartet selection are the
                             reference's either way. */
+    int replicas_per_lane; /* plain sweep on the CTA / cluster kernels
+                            (cluster_size >= 1): 2 or 3 replicas per lane, so
+                            one block is 64 or 96 replicas of a sample and
+                            every staged coupling serves them all; 1: one
+                            replica per lane; 0 (default): 1 until
+                            pspin_autotune_lanes picks it.  The chain is the
+                            same for every value (same summation order per
+                            replica). */
 } pspin_options;
 
 typedef struct pspin_info {
@@ -283,8 +291,14 @@ int  pspin_pt_shape(pspin_state* s, int* NT, int* nrep_per_temp, int* pt_freq);
  * own samples, restoring amplitudes, energies, counters and the sweep index
  * after each trial, and keeps the fastest for the current proposal.
  * ms_per_sweep[6][4] (or NULL) receives the timings, -1 where a shape does
- * not fit or does not apply; *chosen_cluster 0 means the resident kernel. */
+ * not fit or does not apply; *chosen_cluster 0 means the resident kernel.
+ * The plain sweep keeps its current replicas per lane. */
 int  pspin_autotune(pspin_state* s, int sweeps, int* chosen_warps, int* chosen_cluster, float* ms_per_sweep);
+/* The same for the plain sweep over 1, 2 and 3 replicas per lane as well:
+ * ms_per_sweep[3][6][4] (replicas per lane 1..3, then as above; the resident
+ * row applies only to 1).  The chain does not depend on the choice. */
+int  pspin_autotune_lanes(pspin_state* s, int sweeps, int* chosen_warps, int* chosen_cluster,
+                          int* chosen_replicas_per_lane, float* ms_per_sweep);
 /* Observable series at one temperature slot (no reference counterpart; the
  * reference writes E every save_freq sweeps to energy_accept.txt and
  * configurations to configs.bin, parallel_tempering.cu:355-416).  After
