@@ -10,7 +10,8 @@ written by tests/golden/time_reference.py on the same kind of GPU).
      one sample (seed 42, the reference's run) and 64 samples (seeds 42..105)
 (3, the batched workload, is bench.py's.)
 
-Each run: set-up, a few warm-up sweeps, the block-shape autotuner, then a
+Each run: set-up, a few warm-up sweeps, the block-shape autotuner (block
+shape and replicas per lane, pspin_autotune_lanes), then a
 timed run of device-resident sweeps (PT cycles replayed as CUDA graphs) with
 the wall clock around the synchronous calls.  Rate = replicas x N/2 x sweeps
 / seconds (pair-moves/s), the reference's unit.
@@ -39,14 +40,14 @@ REF_KEYS = {"1": "config1_dense_pt_n32_fmc2", "2": "config2_sparse_pt_n512_comb"
             "5": "config5_dense_pt_n64_fmc2"}
 
 
-def _pt_engine(N, seeds, NT, nrep, variant, fmc, gamma, shape, Tmin=0.2, Tmax=1.6):
+def _pt_engine(N, seeds, NT, nrep, variant, fmc, gamma, shape, Tmin=0.2, Tmax=1.6, stream=False):
     cfgs = []
     for s in seeds:
         c = default_config(N=N, nrep=NT * nrep, seed=s, fmc_mode=fmc)
         c.gamma = gamma
         cfgs.append(c)
     t0 = time.perf_counter()
-    eng = Engine(cfgs, variant, _options(shape))
+    eng = Engine(cfgs, variant, _options(shape, disorder_stream=stream))
     setup = time.perf_counter() - t0
     _, betas = temperature_schedule(NT, Tmin, Tmax, True)
     eng.pt_init(NT, nrep, betas, 1)
@@ -54,30 +55,36 @@ def _pt_engine(N, seeds, NT, nrep, variant, fmc, gamma, shape, Tmin=0.2, Tmax=1.
 
 
 def _options(shape, **kw):
-    w, c = shape if shape else (0, None)
+    w, c = shape[:2] if shape else (0, None)
     c = 0 if c is None else (-1 if c == 0 else c)      # 0 from the autotuner: the list-resident kernel
-    return make_options(quiet=True, warps_per_unit=w, cluster_size=c, **kw)
+    k = shape[2] if shape and len(shape) > 2 else 0
+    return make_options(quiet=True, warps_per_unit=w, cluster_size=c, replicas_per_lane=k, **kw)
 
 
 def _timed(eng, run, sweeps, warmup, tune_sweeps, shape):
     run(warmup)
     if shape:
-        w, c = shape
+        w, c = shape[:2]
+        k = shape[2] if len(shape) > 2 else 1
     else:
-        w, c, ms = eng.autotune(tune_sweeps)
+        w, c, k, ms = eng.autotune_lanes(tune_sweeps)
     run(warmup)
     t0 = time.perf_counter()
     run(sweeps)
-    return time.perf_counter() - t0, w, c
+    return time.perf_counter() - t0, w, c, k
 
 
-def measure(config: str, sweeps: int | None = None, shape=None) -> dict:
+def measure(config: str, sweeps: int | None = None, shape=None, stream: bool = False) -> dict:
+    """stream: sparse couplings from per-quartet counter-based normals
+    (options.disorder_stream) instead of the reference's 2*C(N,4) cuRAND
+    normals (45 GB on the device at N=512 during set-up); same law and
+    kernels, not the reference's values."""
     if config == "1":
         eng, setup = _pt_engine(32, [42], 20, 4, PSPIN_DENSE, 2, 0.1, shape)
         sweeps = sweeps or 4096
         run = eng.pt_run
     elif config == "2":
-        eng, setup = _pt_engine(512, [42], 32, 4, PSPIN_SPARSE, 1, 1.0, shape)
+        eng, setup = _pt_engine(512, [42], 32, 4, PSPIN_SPARSE, 1, 1.0, shape, stream=stream)
         sweeps = sweeps or 4096
         run = eng.pt_run
     elif config == "4":
@@ -100,14 +107,14 @@ def measure(config: str, sweeps: int | None = None, shape=None) -> dict:
         raise ValueError(config)
     moves = sum(N * R // 2 for N, R in zip(eng.Ns, eng.Rs))
     chains = sum(eng.Rs)
-    secs, w, cl = _timed(eng, run, sweeps, warmup=8 if config != "4" else 2,
+    secs, w, cl, k = _timed(eng, run, sweeps, warmup=8 if config != "4" else 2,
                          tune_sweeps=2 if config == "4" else 8, shape=shape)
     eng.free()
     rate = moves * sweeps / secs
     # latency-bound configurations: time per move along one replica's chain
     out = {"config": config, "sweeps": sweeps, "seconds": secs, "pair_moves_per_s": rate,
            "chains": chains, "ns_per_move_per_chain": 1e9 * chains / rate,
-           "warps_per_cta": w, "ctas_per_replica_block": cl, "setup_s": setup}
+           "warps_per_cta": w, "ctas_per_replica_block": cl, "replicas_per_lane": k, "setup_s": setup}
     ref = os.path.join(ROOT, "profiles", "reference_sm100_timing.json")
     key = REF_KEYS.get(config)
     if key and os.path.exists(ref):
@@ -172,11 +179,14 @@ def main(argv=None) -> int:
     ap.add_argument("--precision", action="store_true")
     ap.add_argument("--fields", action="store_true", help="tensor-core vs FP64 all-site fields at configuration 4")
     ap.add_argument("--sweeps", type=int, default=0, help="timed sweeps (0: the configuration's default)")
-    ap.add_argument("--shape", default="", help="W,C: warps per CTA and CTAs per replica block (skips the autotuner)")
+    ap.add_argument("--shape", default="", help="W,C[,K]: warps per CTA, CTAs per replica block, replicas per lane "
+                                                "(skips the autotuner)")
+    ap.add_argument("--disorder-stream", action="store_true",
+                    help="configuration 2: streamed sparse couplings (no 45 GB set-up buffer)")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     shape = tuple(int(x) for x in a.shape.split(",")) if a.shape else None
-    res = [measure(k, a.sweeps or None, shape) for k in a.configs.split(",") if k]
+    res = [measure(k, a.sweeps or None, shape, a.disorder_stream) for k in a.configs.split(",") if k]
     if a.precision:
         res.append(precision())
     if a.fields:
