@@ -166,11 +166,16 @@ def run_engine(args, rank, world, device, dist):
         eng.pt_run(sps)
     # block shape by the engine's autotuner (state restored after its trials),
     # then one more step so the PT graph is captured with that shape
+    tuned_table = None
     if shape:
         tuned_w, tuned_c = shape[:2]
         tuned_k = shape[2] if len(shape) > 2 else 1
     else:
         tuned_w, tuned_c, tuned_k, tuned_ms = eng.autotune_lanes(2)
+        # ms per sweep of every shape the tuner ran: "K,C,W" -> ms
+        tuned_table = {f"{k + 1},{c},{w}": round(float(tuned_ms[k, ci, wi]), 3)
+                       for k in range(3) for ci, c in enumerate((0, 1, 2, 4, 8, 16))
+                       for wi, w in enumerate((1, 2, 4, 8)) if tuned_ms[k, ci, wi] > 0}
     eng.pt_run(sps)
     eng.get_profile()                  # zero the launch counters
     ext = torch.cuda.ExternalStream(eng.stream_ptr(), device=device)
@@ -312,7 +317,8 @@ def run_engine(args, rank, world, device, dist):
                    "parallelism": f"samples sharded, {world} GPU(s), no collective",
                    "block_shape": {"warps_per_cta": tuned_w, "ctas_per_replica_block": tuned_c,
                                    "replicas_per_lane": tuned_k,
-                                   "chosen_by": "--shape" if shape else "pspin_autotune_lanes (2 sweeps per shape)"},
+                                   "chosen_by": "--shape" if shape else "pspin_autotune_lanes (2 sweeps per shape)",
+                                   "ms_per_sweep_by_replicas_per_lane_cluster_warps": tuned_table},
                    "launch": "sweep + exchange per PT step, replayed as CUDA graphs of 32 steps",
                    "setup_s": t_setup},
         "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "resync": resync,

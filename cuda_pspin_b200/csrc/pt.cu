@@ -226,8 +226,26 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(float* out, int iters) {
     out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
-cudaError_t launch_fma_probe(float* out, int blocks, int iters, cudaStream_t st) {
-    fma_probe_kernel<<<blocks, 256, 0, st>>>(out, iters);
+// the same with paired FMA (fma.rn.f32x2): 8 chains of two lanes each
+__global__ void __launch_bounds__(256) fma2_probe_kernel(float* out, int iters) {
+    float2 a[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) a[c] = make_float2((float)(threadIdx.x + c) * 1e-3f, (float)(threadIdx.x - c) * 1e-3f);
+    const float2 m = make_float2(0.999999f, 0.999998f), k = make_float2(1e-7f, 2e-7f);
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int c = 0; c < 8; c++) a[c] = __ffma2_rn(a[c], m, k);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < 8; c++) s += a[c].x + a[c].y;
+    out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// paired = 1: the fma.rn.f32x2 probe (twice the FMA per thread and iteration)
+cudaError_t launch_fma_probe(float* out, int blocks, int iters, cudaStream_t st, int paired) {
+    if (paired) fma2_probe_kernel<<<blocks, 256, 0, st>>>(out, iters);
+    else fma_probe_kernel<<<blocks, 256, 0, st>>>(out, iters);
     return cudaGetLastError();
 }
 

@@ -79,12 +79,7 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     const bool writer = rank == 0;
     const int64_t gr = S.rep_off + U.rep_begin + lane;
 
-    for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
-        const int site = idx >> 5, l = idx & 31;
-        float2 v = make_float2(1.f, 0.f);
-        if (l < U.rep_count) v = P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l];
-        sp[idx] = v;
-    }
+    load_block_amplitudes(sp, P.spins + S.spin_off + U.rep_begin, R, N, kRepBlock, U.rep_count);
     if (threadIdx.x < kRepBlock) sp[N * kRepBlock + threadIdx.x] = make_float2(1.f, 0.f);  // virtual site
     if (threadIdx.x == 0) *cflag = 0;
 

@@ -60,6 +60,55 @@ __device__ __forceinline__ void propose(float2 ai, float2 aj, U4 w, float2& ain,
     propose_with<VARIANT>(ai, aj, t, ain, ajn);
 }
 
+// ---------------------------------------------------------------- block state
+// Prologue copies into shared memory with kInFlight independent loads per
+// thread before their stores, so a CTA's state arrives in a few memory
+// latencies rather than one per loop trip.
+constexpr int kInFlight = 8;
+
+// A replica block's amplitudes: columns [0, kb) of rows [0, N) of the
+// sample's [site][R] array `src` (already offset to the block's first
+// replica) into sp[site * kb + col]; columns >= rep_count are 1+0i.
+__device__ __forceinline__ void load_block_amplitudes(float2* sp, const float2* src, int64_t R, int N, int kb,
+                                                      int rep_count) {
+    const int total = N * kb;
+    const int step = (int)blockDim.x;
+    for (int i0 = threadIdx.x; i0 < total; i0 += kInFlight * step) {
+        float2 v[kInFlight];
+#pragma unroll
+        for (int u = 0; u < kInFlight; u++) {
+            const int idx = i0 + u * step;
+            const int site = idx / kb, col = idx - site * kb;
+            v[u] = make_float2(1.f, 0.f);
+            if (idx < total && col < rep_count) v[u] = src[site * R + col];
+        }
+#pragma unroll
+        for (int u = 0; u < kInFlight; u++) {
+            const int idx = i0 + u * step;
+            if (idx < total) sp[idx] = v[u];
+        }
+    }
+}
+
+// n contiguous elements
+template <class T>
+__device__ __forceinline__ void load_block_range(T* dst, const T* src, int64_t n) {
+    const int64_t step = blockDim.x;
+    for (int64_t i0 = threadIdx.x; i0 < n; i0 += kInFlight * step) {
+        T v[kInFlight];
+#pragma unroll
+        for (int u = 0; u < kInFlight; u++) {
+            const int64_t idx = i0 + u * step;
+            if (idx < n) v[u] = src[idx];
+        }
+#pragma unroll
+        for (int u = 0; u < kInFlight; u++) {
+            const int64_t idx = i0 + u * step;
+            if (idx < n) dst[idx] = v[u];
+        }
+    }
+}
+
 // ---------------------------------------------------------------- TMA ring
 // Each warp streams the chunks of its share of the two site lists of every
 // move through a ring of kStages shared-memory slots.  Lane 0 issues 1-D

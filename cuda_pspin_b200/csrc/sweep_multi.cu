@@ -56,12 +56,7 @@ __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P
     int* cflag = reinterpret_cast<int*>(cred + (size_t)2 * CW * KB);
     const bool writer = rank == 0;
 
-    for (int idx = threadIdx.x; idx < N * KB; idx += blockDim.x) {
-        const int site = idx / KB, rr = idx % KB;            // rr = k*32 + lane
-        float2 v = make_float2(1.f, 0.f);
-        if (rr < U.rep_count) v = P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + rr];
-        sp[idx] = v;
-    }
+    load_block_amplitudes(sp, P.spins + S.spin_off + U.rep_begin, R, N, KB, U.rep_count);   // column k*32 + lane
     for (int idx = threadIdx.x; idx < KB; idx += blockDim.x) sp[(size_t)N * KB + idx] = make_float2(1.f, 0.f);
     if (threadIdx.x == 0) *cflag = 0;
 

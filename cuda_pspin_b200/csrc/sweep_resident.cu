@@ -10,8 +10,10 @@
 //
 // Concurrent commuting moves.  With K warps per replica block, the moves
 // are taken in windows of 32: the lanes of warp 0 draw the window's pair
-// picks (one Philox call each) and mark, for every move, the earlier moves
-// of the window it does not commute with -- move b does not commute with
+// picks (one Philox call each), every warp precomputes the random words,
+// sines and cosines of its share of the window's proposals, and the warps
+// mark, for every move, the earlier moves of the window it does not commute
+// with -- move b does not commute with
 // move a when one of b's sites is a site of a or shares a quartet (or a g2
 // term) with one: then b's proposal or fields would read an amplitude that a
 // changes.  The window is cut greedily, in move order, into batches of at
@@ -30,15 +32,14 @@ namespace pspin {
 
 // Shared memory: amplitudes [(N+1)][32] float2 ((N+1)*256 bytes, so the list
 // entries that follow are 16-byte aligned: tiles are read as int4), the
-// sample's list entries, site ranges [N] int2, pair picks [32] int2,
-// conflict masks [32] u32, batch bounds [34] int, per-batch dE and decisions
-// [2][K][32] (float, int), neighbour masks [N][ceil(N/32)] u32 (K > 1 only).
+// sample's list entries, site ranges [N] int2, the window's pair picks and
+// (sweep, step) of each move [32] int2 each, batch bounds [34] int,
+// conflict masks [32] u32, per-batch dE and decisions [2][K][32] (float,
+// int), and the window's precomputed proposal parts [32 moves][7][32] float.
 inline size_t resident_smem_bytes(int N, int64_t entries, int K) {
-    size_t b = (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)entries * sizeof(int2) + (size_t)N * sizeof(int2) +
-               32 * sizeof(int2) + 32 * sizeof(uint32_t) + 34 * sizeof(int) +
-               (size_t)2 * K * kRepBlock * (sizeof(float) + sizeof(int));
-    if (K > 1) b += (size_t)N * ((N + 31) / 32) * sizeof(uint32_t);
-    return b;
+    return (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)entries * sizeof(int2) + (size_t)N * sizeof(int2) +
+           2 * 32 * sizeof(int2) + 34 * sizeof(int) + 32 * sizeof(uint32_t) +
+           (size_t)2 * K * kRepBlock * (sizeof(float) + sizeof(int)) + (size_t)32 * 7 * kRepBlock * sizeof(float);
 }
 
 template <int VARIANT>
@@ -49,7 +50,9 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
     const int N = S.N, R = S.R;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int K = (int)(blockDim.x >> 5);
+    const int owner = K - 1;                   // keeps the running energy and counters
     const int wpr = (N + 31) >> 5;             // words per neighbour-mask row
+    const uint32_t* nbm = P.nbmask + S.nb_off; // read through L1
     const int* sc = P.site_chunks + S.split_off;
     const int64_t e0 = __ldg(P.chunk_start + __ldg(sc));
     const int64_t e1 = __ldg(P.chunk_start + __ldg(sc + (int64_t)(N - 1) * (kSplit + 1) + kSplit));
@@ -57,26 +60,20 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
     int2* L = reinterpret_cast<int2*>(sp + (size_t)(N + 1) * kRepBlock);
     int2* rng_site = L + (e1 - e0);
     int2* picks = rng_site + N;
-    uint32_t* cm = reinterpret_cast<uint32_t*>(picks + 32);
-    int* bounds = reinterpret_cast<int*>(cm + 32);             // [0..32] batch starts, [33] batch count
-    float* dEx = reinterpret_cast<float*>(bounds + 34);        // [2][K][32]
+    int2* mk = picks + 32;                                     // (sweep - sweep0, step) of each move
+    int* bounds = reinterpret_cast<int*>(mk + 32);             // [0..32] batch starts, [33] batch count
+    uint32_t* cm = reinterpret_cast<uint32_t*>(bounds + 34);   // [32]
+    float* dEx = reinterpret_cast<float*>(cm + 32);            // [2][K][32]
     int* acx = reinterpret_cast<int*>(dEx + 2 * K * kRepBlock);  // [2][K][32]
-    uint32_t* nbm = reinterpret_cast<uint32_t*>(acx + 2 * K * kRepBlock);
+    float* tr = reinterpret_cast<float*>(acx + 2 * K * kRepBlock);  // [32][7][32]
     for (int m = threadIdx.x; m < N; m += blockDim.x) {
         const int64_t b = __ldg(P.chunk_start + __ldg(sc + (int64_t)m * (kSplit + 1)));
         const int64_t e = __ldg(P.chunk_start + __ldg(sc + (int64_t)m * (kSplit + 1) + kSplit));
         rng_site[m] = make_int2((int)(b - e0), (int)(e - e0));
     }
-    for (int64_t t = threadIdx.x; t < e1 - e0; t += blockDim.x) L[t] = P.entries[e0 + t];
-    for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
-        const int site = idx >> 5, l = idx & 31;
-        float2 v = make_float2(1.f, 0.f);
-        if (l < U.rep_count) v = P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l];
-        sp[idx] = v;
-    }
+    load_block_range(L, P.entries + e0, e1 - e0);
+    load_block_amplitudes(sp, P.spins + S.spin_off + U.rep_begin, R, N, kRepBlock, U.rep_count);
     if (threadIdx.x < kRepBlock) sp[N * kRepBlock + threadIdx.x] = make_float2(1.f, 0.f);   // virtual site
-    if (K > 1)
-        for (int t = threadIdx.x; t < N * wpr; t += blockDim.x) nbm[t] = __ldg(P.nbmask + S.nb_off + t);
 
     const bool active = lane < U.rep_count;
     const int64_t gr = S.rep_off + U.rep_begin + lane;
@@ -90,16 +87,16 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
         const uint64_t key = P.key[gr];
         k0 = (uint32_t)key;
         k1 = (uint32_t)(key >> 32);
-        if (warp == 0) E = P.energy[gr];
+        if (warp == owner) E = P.energy[gr];
     }
     const long long sweep0 = *P.sweep_counter;
     const int steps = N / 2, total = P.nsweeps * steps;
     // is `site` a site of move q or a neighbour of one?
     auto in_reach = [&](int site, int2 q) {
-        return site == q.x || site == q.y || ((nbm[q.x * wpr + (site >> 5)] >> (site & 31)) & 1u) ||
-               ((nbm[q.y * wpr + (site >> 5)] >> (site & 31)) & 1u);
+        return site == q.x || site == q.y || ((__ldg(nbm + q.x * wpr + (site >> 5)) >> (site & 31)) & 1u) ||
+               ((__ldg(nbm + q.y * wpr + (site >> 5)) >> (site & 31)) & 1u);
     };
-    // warp 0's running energy and counters take a batch's moves in move order
+    // the owner warp's running energy and counters take a batch's moves in move order
     auto account = [&](int par, int n) {
         for (int w = 0; w < n; w++) {
             if (acx[(par * K + w) * kRepBlock + lane]) {
@@ -115,58 +112,81 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
     int prev = 0;                              // moves in the previous batch
     for (int m0 = 0; m0 < total; m0 += 32) {
         const int n = min(32, total - m0);
-        if (warp == 0) {                       // the window's pairs and batches
-            int i0 = 0, j0 = 1;
-            if (lane < n)
-                pair_pick(S.pair_key0, S.pair_key1, (uint64_t)(sweep0 + (m0 + lane) / steps),
-                          (uint32_t)((m0 + lane) % steps), N, i0, j0);
+        if (warp == 0) {                       // the window's pairs
+            int i0 = 0, j0 = 1, sw = 0, kk = 0;
+            if (lane < n) {
+                sw = (m0 + lane) / steps;
+                kk = (m0 + lane) % steps;
+                pair_pick(S.pair_key0, S.pair_key1, (uint64_t)(sweep0 + sw), (uint32_t)kk, N, i0, j0);
+            }
             picks[lane] = make_int2(i0, j0);
-            __syncwarp();
-            if (K > 1) {
-                uint32_t mask = 0;
-                for (int j = 0; j < lane && lane < n; j++) {
+            mk[lane] = make_int2(sw, kk);
+            cm[lane] = 0u;
+        }
+        // every warp: the state-independent parts of the proposals of its share
+        // of the window's moves (random words, sines and cosines), for its lanes
+        for (int t = warp; t < n; t += K) {
+            const int m = m0 + t;
+            float tt[7];
+            move_trig<VARIANT>(move_words(k0, k1, (uint64_t)(sweep0 + m / steps), (uint32_t)(m % steps)), tt);
+#pragma unroll
+            for (int q = 0; q < 7; q++) tr[(t * 7 + q) * kRepBlock + lane] = tt[q];
+        }
+        __syncthreads();
+        if (K > 1) {
+            // conflict masks: the earlier moves of the window that move `lane`
+            // does not commute with, the earlier moves shared out over the warps
+            uint32_t part = 0;
+            if (lane < n) {
+                const int2 me = picks[lane];
+                for (int j = warp; j < lane; j += K) {
                     const int2 q = picks[j];
-                    if (in_reach(i0, q) || in_reach(j0, q)) mask |= 1u << j;
+                    if (in_reach(me.x, q) || in_reach(me.y, q)) part |= 1u << j;
                 }
-                cm[lane] = mask;
-                __syncwarp();
+            }
+            if (part) atomicOr(cm + lane, part);
+            __syncthreads();
+            if (warp == 0) {
+                // greedy cut in move order: a batch [s0, e) ends at the first move
+                // that does not commute with one of [s0, itself), or after K moves
+                const uint32_t mask = cm[lane];
+                int nb = 0;
+                for (int s0 = 0; s0 < n;) {
+                    const unsigned bad = __ballot_sync(0xffffffffu, lane > s0 && lane < n && (mask >> s0) != 0u);
+                    const int e = min(bad ? __ffs(bad) - 1 : n, min(n, s0 + K));
+                    if (lane == 0) bounds[nb] = s0;
+                    nb++;
+                    s0 = e;
+                }
                 if (lane == 0) {
-                    int nb = 0;
-                    for (int s0 = 0; s0 < n;) {
-                        int e = s0 + 1;
-                        uint32_t span = 1u << s0;
-                        while (e < n && e - s0 < K && (cm[e] & span) == 0) {
-                            span |= 1u << e;
-                            e++;
-                        }
-                        bounds[nb++] = s0;
-                        s0 = e;
-                    }
                     bounds[nb] = n;
                     bounds[33] = nb;
                 }
-            } else if (lane == 0) {
+            }
+            __syncthreads();
+        } else {
+            if (lane == 0) {
                 for (int b = 0; b <= n; b++) bounds[b] = b;
                 bounds[33] = n;
             }
+            __syncwarp();
         }
-        __syncthreads();
         const int nb = bounds[33];
         for (int b = 0; b < nb; b++) {
             const int bs = bounds[b], be = bounds[b + 1];
             const int par = (int)(batches & 1);
-            if (warp == 0 && batches > 0) account(par ^ 1, prev);
+            if (warp == owner && batches > 0) account(par ^ 1, prev);
             if (warp < be - bs) {
-                const int m = m0 + bs + warp;
-                const long long sw = sweep0 + m / steps;
-                const int k = m % steps;
-                const int2 pq = picks[bs + warp];
+                const int t = bs + warp;
+                const int2 pq = picks[t], swk = mk[t];
                 const int i0 = pq.x, j0 = pq.y;
-                const U4 w = move_words(k0, k1, (uint64_t)sw, (uint32_t)k);
+                float tt[7];
+#pragma unroll
+                for (int q = 0; q < 7; q++) tt[q] = tr[(t * 7 + q) * kRepBlock + lane];
                 const float2 ai = sp[i0 * kRepBlock + lane], aj = sp[j0 * kRepBlock + lane];
                 float2 ain, ajn;
-                propose<VARIANT>(ai, aj, w, ain, ajn);
-                const float cu = u01f(w.w);
+                propose_with<VARIANT>(ai, aj, tt, ain, ajn);
+                const float cu = tt[6];
                 sp[j0 * kRepBlock + lane] = ajn;       // h_i is evaluated at the proposed a_j
                 __syncwarp();
                 float hix = 0.f, hiy = 0.f, hjx = 0.f, hjy = 0.f;
@@ -190,7 +210,7 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
                 dEx[(par * K + warp) * kRepBlock + lane] = dE;
                 acx[(par * K + warp) * kRepBlock + lane] = accept ? 1 : 0;
                 if (P.trace != nullptr && U.sample == P.trace_sample && U.rep_begin + lane == P.trace_rep && active) {
-                    const long long idx = (sw - P.trace_sweep0) * steps + k;
+                    const long long idx = (long long)swk.x * steps + swk.y + (sweep0 - P.trace_sweep0) * steps;
                     if (idx >= 0 && idx < P.trace_cap) {
                         pspin_move_record* rec = reinterpret_cast<pspin_move_record*>(P.trace) + idx;
                         rec->i0 = i0; rec->j0 = j0;
@@ -210,12 +230,12 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
             batches++;
         }
     }
-    if (warp == 0 && batches > 0) account((int)((batches - 1) & 1), prev);
+    if (warp == owner && batches > 0) account((int)((batches - 1) & 1), prev);
     for (int idx = threadIdx.x; idx < N * kRepBlock; idx += blockDim.x) {
         const int site = idx >> 5, l = idx & 31;
         if (l < U.rep_count) P.spins[S.spin_off + (int64_t)site * R + U.rep_begin + l] = sp[idx];
     }
-    if (warp == 0 && active) {
+    if (warp == owner && active) {
         P.energy[gr] = E;
         P.accepted[gr] += nacc;
         P.proposed[gr] += nprop;

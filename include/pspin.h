@@ -426,8 +426,9 @@ int  pspin_get_profile(pspin_state* s, double* sweep_kernel_ms, int64_t* sweep_l
  * lists (about 4 per quartet term and replica) plus the same 64 per move.
  * Either pointer may be NULL. */
 int  pspin_sweep_work(pspin_state* s, double* algorithmic_flops, double* executed_flops);
-/* FP32 FMA throughput of the current device (TFLOP/s), measured by a
- * register-resident FMA loop over all SMs: the roofline denominator of the
+/* FP32 FMA throughput of the current device (TFLOP/s), measured by
+ * register-resident FMA loops over all SMs, scalar and paired
+ * (fma.rn.f32x2), the faster of the two: the roofline denominator of the
  * FP32 sweep. */
 int  pspin_fp32_peak(double* tflops);
 
