@@ -283,6 +283,17 @@ double list_exec_flops(const SiteLists& L, int N, bool tiles) {
     return total;
 }
 
+bool lists_single_groups(const SiteLists& L) {
+    const int64_t nchunks = (int64_t)L.chunk_start.size();
+    for (int64_t c = 0; c < nchunks; c++) {
+        const int64_t b = L.chunk_start[c];
+        const int64_t e = (c + 1 < nchunks) ? L.chunk_start[c + 1] : (int64_t)L.entries.size();
+        for (int64_t u = b; u < e; u += 2)
+            if (L.entries[u].x != 1) return false;
+    }
+    return true;
+}
+
 void build_q64(const std::vector<QuartetRec>& qs, std::vector<Q64>& out) {
     out.resize(qs.size());
     for (size_t t = 0; t < qs.size(); t++) {

@@ -44,8 +44,10 @@ __host__ __device__ inline size_t cluster_pre_offset(int N, int warps) {
 __host__ __device__ inline size_t cluster_buffer_offset(int N, int warps) {
     return (cluster_pre_offset(N, warps) + (size_t)2 * 7 * kRepBlock * sizeof(float) + 15) & ~(size_t)15;
 }
+// (+ kStaticSmem: the ring tags are static shared memory, counted here so
+// that every fit check against the 227 KB a CTA can have includes them)
 inline size_t cluster_smem_bytes(int N, int warps, int C) {
-    return cluster_buffer_offset(N, warps) + (size_t)2 * C * warps * kRepBlock * sizeof(float4) + 16;
+    return cluster_buffer_offset(N, warps) + (size_t)2 * C * warps * kRepBlock * sizeof(float4) + 16 + kStaticSmem;
 }
 
 __device__ __forceinline__ void add4(float4& a, const float4 b) {
@@ -122,12 +124,17 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     Cursor pc = st.first();
     uint32_t issued = 0, consumed = 0;
     bool ok = true;
+    // each ring slot's tag: {move * 2 + list, entries}, written by lane 0 when
+    // the copy is issued, so the consumer needs no list lookups of its own
+    __shared__ int2 rtag_all[8 * kStages];
+    int2* rtag = rtag_all + warp * kStages;
     auto issue = [&]() {
         if (pc.m >= total) return;
         const uint32_t slot = issued % kStages;
         if (lane == 0) {
             const int64_t b = __ldg(P.chunk_start + pc.c), e = __ldg(P.chunk_start + pc.c + 1);
             const uint32_t bytes = (uint32_t)((e - b) * sizeof(int2));
+            rtag[slot] = make_int2(pc.m * 2 + pc.which, (int)(e - b));
             mbar_expect_tx(bars + slot, bytes);
             bulk_g2s(ring + slot * kStage, P.entries + b, bytes, bars + slot);
         }
@@ -183,21 +190,26 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
         // ---- field pass m
         float h[4] = {0.f, 0.f, 0.f, 0.f};
         if (m == P.stall_move) ok = stall_wait(&stall_bar, P.status, P.wait_clocks);
-        for (int which = 0; which < 2 && ok; which++) {
-            int c, c_end;
-            st.range(m, which, c, c_end);
-            for (; c < c_end; c++) {
-                const uint32_t slot = consumed % kStages;
-                ok = ring_wait(bars + slot, (consumed / kStages) & 1u, P.status, P.wait_clocks);
-                if (!ok) break;                    // stop consuming and issuing; abort below
-                const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
-                if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
-                else accumulate_chunk(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
-                consumed++;
-                __syncwarp();
-                if (lane == 0) fence_async_shared();
-                issue();
+        // the ring's chunks tagged with move m, in issue order: site i0's list, then j0's
+        while (ok) {
+            __syncwarp();
+            if (consumed == issued) break;
+            const uint32_t slot = consumed % kStages;
+            const int2 tg = rtag[slot];
+            if ((tg.x >> 1) != m) break;
+            ok = ring_wait(bars + slot, (consumed / kStages) & 1u, P.status, P.wait_clocks);
+            if (!ok) break;                        // stop consuming and issuing; abort below
+            if (tg.x & 1) {
+                if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
+                else accumulate_chunk(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
+            } else {
+                if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
+                else accumulate_chunk(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
             }
+            consumed++;
+            __syncwarp();
+            if (lane == 0) fence_async_shared();
+            issue();
         }
         // the next move's pair and its sites' amplitudes in the state the
         // field pass just read (this move's decision can change only ci0, cj0)

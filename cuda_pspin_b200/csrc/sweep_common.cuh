@@ -60,6 +60,10 @@ __device__ __forceinline__ void propose(float2 ai, float2 aj, U4 w, float2& ain,
     propose_with<VARIANT>(ai, aj, t, ain, ajn);
 }
 
+// Static shared memory of the ring-fed cluster kernels (ring tags, the
+// stall-test barrier), kept free in their dynamic-size accounting.
+constexpr size_t kStaticSmem = 256;
+
 // ---------------------------------------------------------------- block state
 // Prologue copies into shared memory with kInFlight independent loads per
 // thread before their stores, so a CTA's state arrives in a few memory
@@ -279,6 +283,33 @@ __device__ __forceinline__ void accumulate_chunk(const int2* __restrict__ R, int
         hx = fmaf(px, yx, fmaf(-py, yy, hx));
         hy = fmaf(px, yy, fmaf(py, yx, hy));
         e += len + 1;
+    }
+}
+
+// The same for lists whose groups all have one data entry, read as 16-byte
+// records {1, p<<16|o1, g, o2} with no dependence of one record's position
+// on the previous header, so the records' loads overlap.  The arithmetic is
+// accumulate_chunk's for a group of one entry, so the result is bit for bit
+// the same.
+template <int kUnroll = 4>
+__device__ __forceinline__ void accumulate_flat(const int2* __restrict__ R2, int n,
+                                                const float2* __restrict__ sp, int lane,
+                                                float& hx, float& hy) {
+    const int4* __restrict__ R = reinterpret_cast<const int4*>(R2);
+    const int nr = n >> 1;
+#pragma unroll kUnroll
+    for (int r = 0; r < nr; r++) {
+        const int4 q = R[r];
+        const int p = q.y >> 16, o1 = q.y & 0xFFFF;
+        const float2 ap = sp[p * kRepBlock + lane];
+        const float2 ao = sp[o1 * kRepBlock + lane];
+        const float2 a = sp[q.w * kRepBlock + lane];
+        const float g = __int_as_float(q.z);
+        const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
+        const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
+        const float yx = fmaf(g, a.x, 0.f), yy = fmaf(-g, a.y, 0.f);
+        hx = fmaf(px, yx, fmaf(-py, yy, hx));
+        hy = fmaf(px, yy, fmaf(py, yx, hy));
     }
 }
 

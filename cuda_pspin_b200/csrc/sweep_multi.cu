@@ -27,8 +27,8 @@ __host__ __device__ inline size_t multi_pre_offset(int N, int W, int K) {
 __host__ __device__ inline size_t multi_buffer_offset(int N, int W, int K) {
     return (multi_pre_offset(N, W, K) + (size_t)2 * 7 * K * kRepBlock * sizeof(float) + 15) & ~(size_t)15;
 }
-inline size_t multi_smem_bytes(int N, int W, int C, int K) {
-    return multi_buffer_offset(N, W, K) + (size_t)2 * C * W * K * kRepBlock * sizeof(float4) + 16;
+inline size_t multi_smem_bytes(int N, int W, int C, int K) {   // + the static ring tags
+    return multi_buffer_offset(N, W, K) + (size_t)2 * C * W * K * kRepBlock * sizeof(float4) + 16 + kStaticSmem;
 }
 
 __device__ __forceinline__ void add4m(float4& a, const float4 b) {
@@ -106,12 +106,17 @@ __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P
     Cursor pc = st.first();
     uint32_t issued = 0, consumed = 0;
     bool ok = true;
+    // each ring slot's tag: {move * 2 + list, entries}, written by lane 0 when
+    // the copy is issued, so the consumer needs no list lookups of its own
+    __shared__ int2 rtag_all[8 * kStages];
+    int2* rtag = rtag_all + warp * kStages;
     auto issue = [&]() {
         if (pc.m >= total) return;
         const uint32_t slot = issued % kStages;
         if (lane == 0) {
             const int64_t b = __ldg(P.chunk_start + pc.c), e = __ldg(P.chunk_start + pc.c + 1);
             const uint32_t bytes = (uint32_t)((e - b) * sizeof(int2));
+            rtag[slot] = make_int2(pc.m * 2 + pc.which, (int)(e - b));
             mbar_expect_tx(bars + slot, bytes);
             bulk_g2s(ring + slot * kStage, P.entries + b, bytes, bars + slot);
         }
@@ -176,26 +181,26 @@ __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P
 #pragma unroll
         for (int k = 0; k < K; k++) hix[k] = hiy[k] = hjx[k] = hjy[k] = 0.f;
         if (m == P.stall_move) ok = stall_wait(&stall_bar, P.status, P.wait_clocks);
-        for (int which = 0; which < 2 && ok; which++) {
-            int c, c_end;
-            st.range(m, which, c, c_end);
-            for (; c < c_end; c++) {
-                const uint32_t slot = consumed % kStages;
-                ok = ring_wait(bars + slot, (consumed / kStages) & 1u, P.status, P.wait_clocks);
-                if (!ok) break;
-                const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
-                if (which == 0) {
-                    if (S.fc_tiles) accumulate_tiles_k<K, 4>(ring + slot * kStage, n, sp, lane, hix, hiy);
-                    else accumulate_chunk_k<K>(ring + slot * kStage, n, sp, lane, hix, hiy);
-                } else {
-                    if (S.fc_tiles) accumulate_tiles_k<K, 4>(ring + slot * kStage, n, sp, lane, hjx, hjy);
-                    else accumulate_chunk_k<K>(ring + slot * kStage, n, sp, lane, hjx, hjy);
-                }
-                consumed++;
-                __syncwarp();
-                if (lane == 0) fence_async_shared();
-                issue();
+        // the ring's chunks tagged with move m, in issue order: site i0's list, then j0's
+        while (ok) {
+            __syncwarp();
+            if (consumed == issued) break;
+            const uint32_t slot = consumed % kStages;
+            const int2 tg = rtag[slot];
+            if ((tg.x >> 1) != m) break;
+            ok = ring_wait(bars + slot, (consumed / kStages) & 1u, P.status, P.wait_clocks);
+            if (!ok) break;
+            if ((tg.x & 1) == 0) {
+                if (S.fc_tiles) accumulate_tiles_k<K, 4>(ring + slot * kStage, tg.y, sp, lane, hix, hiy);
+                else accumulate_chunk_k<K>(ring + slot * kStage, tg.y, sp, lane, hix, hiy);
+            } else {
+                if (S.fc_tiles) accumulate_tiles_k<K, 4>(ring + slot * kStage, tg.y, sp, lane, hjx, hjy);
+                else accumulate_chunk_k<K>(ring + slot * kStage, tg.y, sp, lane, hjx, hjy);
             }
+            consumed++;
+            __syncwarp();
+            if (lane == 0) fence_async_shared();
+            issue();
         }
         // the next move's pair and its sites' amplitudes in the state the field
         // pass read (move m's decision can change only ci0, cj0)

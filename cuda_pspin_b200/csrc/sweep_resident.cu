@@ -35,11 +35,14 @@ namespace pspin {
 // sample's list entries, site ranges [N] int2, the window's pair picks and
 // (sweep, step) of each move [32] int2 each, batch bounds [34] int,
 // conflict masks [32] u32, per-batch dE and decisions [2][K][32] (float,
-// int), and the window's precomputed proposal parts [32 moves][7][32] float.
+// int), the window's precomputed proposal parts [32 moves][7][32] float,
+// and (K > 1) the neighbour-mask rows of the window's pairs [32][2][ceil(N/32)].
 inline size_t resident_smem_bytes(int N, int64_t entries, int K) {
-    return (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)entries * sizeof(int2) + (size_t)N * sizeof(int2) +
-           2 * 32 * sizeof(int2) + 34 * sizeof(int) + 32 * sizeof(uint32_t) +
-           (size_t)2 * K * kRepBlock * (sizeof(float) + sizeof(int)) + (size_t)32 * 7 * kRepBlock * sizeof(float);
+    size_t b = (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)entries * sizeof(int2) +
+               (size_t)N * sizeof(int2) + 2 * 32 * sizeof(int2) + 34 * sizeof(int) + 32 * sizeof(uint32_t) +
+               (size_t)2 * K * kRepBlock * (sizeof(float) + sizeof(int)) + (size_t)32 * 7 * kRepBlock * sizeof(float);
+    if (K > 1) b += (size_t)64 * ((N + 31) / 32) * sizeof(uint32_t);
+    return b;
 }
 
 template <int VARIANT>
@@ -66,6 +69,7 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
     float* dEx = reinterpret_cast<float*>(cm + 32);            // [2][K][32]
     int* acx = reinterpret_cast<int*>(dEx + 2 * K * kRepBlock);  // [2][K][32]
     float* tr = reinterpret_cast<float*>(acx + 2 * K * kRepBlock);  // [32][7][32]
+    uint32_t* nrow = reinterpret_cast<uint32_t*>(tr + 32 * 7 * kRepBlock);   // [32][2][wpr]
     for (int m = threadIdx.x; m < N; m += blockDim.x) {
         const int64_t b = __ldg(P.chunk_start + __ldg(sc + (int64_t)m * (kSplit + 1)));
         const int64_t e = __ldg(P.chunk_start + __ldg(sc + (int64_t)m * (kSplit + 1) + kSplit));
@@ -91,10 +95,11 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
     }
     const long long sweep0 = *P.sweep_counter;
     const int steps = N / 2, total = P.nsweeps * steps;
-    // is `site` a site of move q or a neighbour of one?
-    auto in_reach = [&](int site, int2 q) {
-        return site == q.x || site == q.y || ((__ldg(nbm + q.x * wpr + (site >> 5)) >> (site & 31)) & 1u) ||
-               ((__ldg(nbm + q.y * wpr + (site >> 5)) >> (site & 31)) & 1u);
+    // is `site` a site of the window's move j or a neighbour of one?
+    auto in_reach = [&](int site, int j) {
+        const int2 q = picks[j];
+        const uint32_t* rows = nrow + 2 * j * wpr;
+        return site == q.x || site == q.y || (((rows[site >> 5] | rows[wpr + (site >> 5)]) >> (site & 31)) & 1u);
     };
     // the owner warp's running energy and counters take a batch's moves in move order
     auto account = [&](int par, int n) {
@@ -134,15 +139,34 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
         }
         __syncthreads();
         if (K > 1) {
+            // the neighbour-mask rows of the window's sites, all loads in flight at once
+            const int tot = n * 2 * wpr;
+            for (int i0 = threadIdx.x; i0 < tot; i0 += kInFlight * blockDim.x) {
+                uint32_t v[kInFlight];
+#pragma unroll
+                for (int u = 0; u < kInFlight; u++) {
+                    const int idx = i0 + u * (int)blockDim.x;
+                    v[u] = 0u;
+                    if (idx < tot) {
+                        const int j = idx / (2 * wpr), r = idx - j * 2 * wpr;
+                        const int2 q = picks[j];
+                        v[u] = __ldg(nbm + (r < wpr ? q.x * wpr + r : q.y * wpr + (r - wpr)));
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kInFlight; u++) {
+                    const int idx = i0 + u * (int)blockDim.x;
+                    if (idx < tot) nrow[idx] = v[u];
+                }
+            }
+            __syncthreads();
             // conflict masks: the earlier moves of the window that move `lane`
             // does not commute with, the earlier moves shared out over the warps
             uint32_t part = 0;
             if (lane < n) {
                 const int2 me = picks[lane];
-                for (int j = warp; j < lane; j += K) {
-                    const int2 q = picks[j];
-                    if (in_reach(me.x, q) || in_reach(me.y, q)) part |= 1u << j;
-                }
+                for (int j = warp; j < lane; j += K)
+                    if (in_reach(me.x, j) || in_reach(me.y, j)) part |= 1u << j;
             }
             if (part) atomicOr(cm + lane, part);
             __syncthreads();
@@ -194,6 +218,9 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
                 if (S.fc_tiles) {
                     accumulate_tiles(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
                     accumulate_tiles(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
+                } else if (S.flat_groups) {
+                    accumulate_flat(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
+                    accumulate_flat(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
                 } else {
                     accumulate_chunk(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
                     accumulate_chunk(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);

@@ -117,14 +117,21 @@ def run(args) -> dict:
         eng.set_proposal(PROPOSAL_PLAIN)
         out["training"]["extra_equilibration_sweeps"] = args.equilibrate
         run_pt(eng, args.equilibrate)
-    # each proposal's kernel gets its own block shape from the autotuner
+    # each proposal's kernel gets its own block shape from the autotuner; the
+    # plain sweep also its replicas per lane (1, 2 or 3)
     shapes = {}
     for prop, name in ((PROPOSAL_PLAIN_FIELDS, "plain_two_pass"), (PROPOSAL_PLAIN, "plain"),
                        (PROPOSAL_LEARNED, "learned")):
         eng.set_proposal(prop)
-        w, c, ms = eng.autotune(4)
-        shapes[name] = {"warps_per_cta": w, "ctas_per_replica_block": c,
-                        "ms_per_sweep_resident_c1_c2_c4_c8_c16_by_warps_1_2_4_8": np.round(ms, 3).tolist()}
+        if prop == PROPOSAL_PLAIN:
+            w, c, k, ms = eng.autotune_lanes(4)
+            shapes[name] = {"warps_per_cta": w, "ctas_per_replica_block": c, "replicas_per_lane": k,
+                            "ms_per_sweep_by_replicas_per_lane_resident_c1_c2_c4_c8_c16_by_warps_1_2_4_8":
+                                np.round(ms, 3).tolist()}
+        else:
+            w, c, ms = eng.autotune(4)
+            shapes[name] = {"warps_per_cta": w, "ctas_per_replica_block": c,
+                            "ms_per_sweep_resident_c1_c2_c4_c8_c16_by_warps_1_2_4_8": np.round(ms, 3).tolist()}
     out["block_shapes"] = shapes
     # interleaved blocks in ABBA order: a slow drift of the samples (ageing)
     # enters both proposals alike
