@@ -24,8 +24,10 @@
 //      reads, and each lane reads only its own replica's column, so the
 //      warps need no barrier between deciding and reading.
 // The state-independent part of a proposal (random words, sines and
-// cosines) is computed one move ahead by the last warp of each CTA into a
-// buffer double-buffered by move parity, as is the exchange buffer: no warp
+// cosines) is computed for windows of kWin moves, a window ahead, by all
+// warps of each CTA at once (warp w the window's moves w, w+W, ...), into a
+// buffer double-buffered by window, so no warp carries that work alone at
+// every move; the exchange buffer is double-buffered by move parity: no warp
 // can be more than one move ahead of another (the barrier of each move
 // waits for all of them).  Rank 0 writes the results back.
 #include "sweep_common.cuh"
@@ -33,16 +35,18 @@
 
 namespace pspin {
 
+constexpr int kWin = 8;    // moves per window of precomputed proposal parts
+
 // Shared memory of one CTA: amplitudes [(N+1)][32] float2; TMA rings
 // [W][kStages][kStage] int2; ring mbarriers [W][kStages]; the precomputed
-// proposal parts [2][7][32] float; then, at a 16-byte boundary, the
+// proposal parts [2][kWin][7][32] float; then, at a 16-byte boundary, the
 // exchange buffer [2][C*W][32] float4 and the cluster's abort flag.
 __host__ __device__ inline size_t cluster_pre_offset(int N, int warps) {
     return (size_t)(N + 1) * kRepBlock * sizeof(float2) + (size_t)warps * kStages * kStage * sizeof(int2) +
            (size_t)warps * kStages * sizeof(uint64_t);
 }
 __host__ __device__ inline size_t cluster_buffer_offset(int N, int warps) {
-    return (cluster_pre_offset(N, warps) + (size_t)2 * 7 * kRepBlock * sizeof(float) + 15) & ~(size_t)15;
+    return (cluster_pre_offset(N, warps) + (size_t)2 * kWin * 7 * kRepBlock * sizeof(float) + 15) & ~(size_t)15;
 }
 // (+ kStaticSmem: the ring tags are static shared memory, counted here so
 // that every fit check against the 227 KB a CTA can have includes them)
@@ -67,13 +71,12 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     const int warp = threadIdx.x >> 5;
     const int W = P.warps;
     const int CW = C * W;
-    const int helper = W - 1;                  // computes the proposal parts one move ahead
     float2* sp = reinterpret_cast<float2*>(smem_raw);                          // [(N+1)][32]
     int2* ring_all = reinterpret_cast<int2*>(sp + (size_t)(N + 1) * kRepBlock);
     int2* ring = ring_all + (size_t)warp * kStages * kStage;
     uint64_t* bars_all = reinterpret_cast<uint64_t*>(ring_all + (size_t)W * kStages * kStage);
     uint64_t* bars = bars_all + warp * kStages;
-    float* pre = reinterpret_cast<float*>(smem_raw + cluster_pre_offset(N, W));        // [2][7][32]
+    float* pre = reinterpret_cast<float*>(smem_raw + cluster_pre_offset(N, W));        // [2][kWin][7][32]
     float4* cred = reinterpret_cast<float4*>(smem_raw + cluster_buffer_offset(N, W));  // [2][C*W][32]
     int* cflag = reinterpret_cast<int*>(cred + (size_t)2 * CW * kRepBlock);            // cluster abort flag
 
@@ -143,14 +146,18 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     };
     for (int s = 0; s < kStages; s++) issue();
 
-    // the helper warp: random words, sines and cosines of move m into pre[m & 1]
-    auto make_pre = [&](int m) {
-        const long long sw = sweep0 + m / steps;
-        float t[7];
-        move_trig<VARIANT>(move_words(k0, k1, (uint64_t)sw, (uint32_t)(m % steps)), t);
-        float* dst = pre + (m & 1) * 7 * kRepBlock;
+    // random words, sines and cosines of the moves of window wn, shared out
+    // over the CTA's warps, into pre[wn & 1]
+    auto make_window = [&](int wn) {
+        for (int t = warp; t < kWin; t += W) {
+            const int m = wn * kWin + t;
+            if (m >= total) break;
+            float tt[7];
+            move_trig<VARIANT>(move_words(k0, k1, (uint64_t)(sweep0 + m / steps), (uint32_t)(m % steps)), tt);
+            float* dst = pre + ((wn & 1) * kWin + t) * 7 * kRepBlock;
 #pragma unroll
-        for (int q = 0; q < 7; q++) dst[q * kRepBlock + lane] = t[q];
+            for (int q = 0; q < 7; q++) dst[q * kRepBlock + lane] = tt[q];
+        }
     };
     auto pair_of = [&](int m, int& i0, int& j0) {
         pair_pick(S.pair_key0, S.pair_key1, (uint64_t)(sweep0 + m / steps), (uint32_t)(m % steps), N, i0, j0);
@@ -160,7 +167,7 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     float2 cai = make_float2(0.f, 0.f), caj = cai, cain = cai, cajn = cai;
     float cu = 0.f;
     auto take_pre = [&](int m, float2 ai, float2 aj) {
-        const float* src = pre + (m & 1) * 7 * kRepBlock;
+        const float* src = pre + (((m / kWin) & 1) * kWin + m % kWin) * 7 * kRepBlock;
         float t[7];
 #pragma unroll
         for (int q = 0; q < 7; q++) t[q] = src[q * kRepBlock + lane];
@@ -175,7 +182,8 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
         mbar_init(&stall_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == helper && total > 0) make_pre(0);
+    make_window(0);
+    make_window(1);
     __syncthreads();
     if (total > 0) {
         pair_of(0, ci0, cj0);
@@ -186,7 +194,10 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
 
     bool aborted = false;
     for (int m = 0; m < total; m++) {
-        if (warp == helper && m + 1 < total) make_pre(m + 1);
+        // window w+1 during the first move of window w: its buffer's last
+        // reader, take_pre at the end of move kWin*w - 2, is behind every
+        // warp that has passed barrier kWin*w - 1
+        if (m >= kWin && m % kWin == 0) make_window(m / kWin + 1);
         // ---- field pass m
         float h[4] = {0.f, 0.f, 0.f, 0.f};
         if (m == P.stall_move) ok = stall_wait(&stall_bar, P.status, P.wait_clocks);

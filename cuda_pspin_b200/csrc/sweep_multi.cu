@@ -5,7 +5,8 @@
 //
 // Same moves, RNG streams and Metropolis rule as sweep_kernel and
 // sweep_cluster_kernel, organised as the latter (one barrier per move, every
-// warp decides, the last warp precomputes the next move's random parts).
+// warp decides, all warps precompute the random parts of a window of moves
+// a window ahead).
 // What K changes: every staged coupling, broadcast from shared memory, is
 // used for the lane's K replicas, so per FFMA there are K times fewer
 // coupling loads, K times more independent accumulator chains per warp, and
@@ -16,16 +17,18 @@
 
 namespace pspin {
 
+constexpr int kWinK = 4;   // moves per window of precomputed proposal parts
+
 // Shared memory of one CTA: amplitudes [(N+1)][K][32] float2; TMA rings
 // [W][kStages][kStage] int2; ring mbarriers [W][kStages]; the precomputed
-// proposal parts [2][7][K][32] float; at a 16-byte boundary the exchange
-// buffer [2][C*W][K][32] float4 and the cluster's abort flag.
+// proposal parts [2][kWinK][7][K][32] float; at a 16-byte boundary the
+// exchange buffer [2][C*W][K][32] float4 and the cluster's abort flag.
 __host__ __device__ inline size_t multi_pre_offset(int N, int W, int K) {
     return (size_t)(N + 1) * K * kRepBlock * sizeof(float2) + (size_t)W * kStages * kStage * sizeof(int2) +
            (size_t)W * kStages * sizeof(uint64_t);
 }
 __host__ __device__ inline size_t multi_buffer_offset(int N, int W, int K) {
-    return (multi_pre_offset(N, W, K) + (size_t)2 * 7 * K * kRepBlock * sizeof(float) + 15) & ~(size_t)15;
+    return (multi_pre_offset(N, W, K) + (size_t)2 * kWinK * 7 * K * kRepBlock * sizeof(float) + 15) & ~(size_t)15;
 }
 inline size_t multi_smem_bytes(int N, int W, int C, int K) {   // + the static ring tags
     return multi_buffer_offset(N, W, K) + (size_t)2 * C * W * K * kRepBlock * sizeof(float4) + 16 + kStaticSmem;
@@ -44,14 +47,14 @@ __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P
     const SampleDev S = P.samples[U.sample];
     const int N = S.N, R = S.R;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int W = P.warps, CW = C * W, helper = W - 1;
+    const int W = P.warps, CW = C * W;
     const int KB = K * kRepBlock;              // replicas of the unit
     float2* sp = reinterpret_cast<float2*>(smem_raw);                              // [(N+1)][K][32]
     int2* ring_all = reinterpret_cast<int2*>(sp + (size_t)(N + 1) * KB);
     int2* ring = ring_all + (size_t)warp * kStages * kStage;
     uint64_t* bars_all = reinterpret_cast<uint64_t*>(ring_all + (size_t)W * kStages * kStage);
     uint64_t* bars = bars_all + warp * kStages;
-    float* pre = reinterpret_cast<float*>(smem_raw + multi_pre_offset(N, W, K));      // [2][7][K][32]
+    float* pre = reinterpret_cast<float*>(smem_raw + multi_pre_offset(N, W, K));      // [2][kWinK][7][K][32]
     float4* cred = reinterpret_cast<float4*>(smem_raw + multi_buffer_offset(N, W, K)); // [2][C*W][K][32]
     int* cflag = reinterpret_cast<int*>(cred + (size_t)2 * CW * KB);
     const bool writer = rank == 0;
@@ -125,17 +128,21 @@ __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P
     };
     for (int s = 0; s < kStages; s++) issue();
 
-    // the helper warp: random words, sines and cosines of move m for the
-    // lane's K replicas into pre[m & 1]
-    auto make_pre = [&](int m) {
-        const long long sw = sweep0 + m / steps;
-        float* dst = pre + (m & 1) * 7 * KB;
+    // random words, sines and cosines of the moves of window wn for the
+    // lane's K replicas, shared out over the CTA's warps, into pre[wn & 1]
+    auto make_window = [&](int wn) {
+        for (int t = warp; t < kWinK; t += W) {
+            const int m = wn * kWinK + t;
+            if (m >= total) break;
+            const long long sw = sweep0 + m / steps;
+            float* dst = pre + ((wn & 1) * kWinK + t) * 7 * KB;
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            float t[7];
-            move_trig<VARIANT>(move_words(k0[k], k1[k], (uint64_t)sw, (uint32_t)(m % steps)), t);
+            for (int k = 0; k < K; k++) {
+                float tt[7];
+                move_trig<VARIANT>(move_words(k0[k], k1[k], (uint64_t)sw, (uint32_t)(m % steps)), tt);
 #pragma unroll
-            for (int q = 0; q < 7; q++) dst[(q * K + k) * kRepBlock + lane] = t[q];
+                for (int q = 0; q < 7; q++) dst[(q * K + k) * kRepBlock + lane] = tt[q];
+            }
         }
     };
     auto pair_of = [&](int m, int& i0, int& j0) {
@@ -145,7 +152,7 @@ __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P
     float2 cai[K], caj[K], cain[K], cajn[K];
     float cu[K];
     auto take_pre = [&](int m, int k, float2 ai, float2 aj) {
-        const float* src = pre + (m & 1) * 7 * KB;
+        const float* src = pre + (((m / kWinK) & 1) * kWinK + m % kWinK) * 7 * KB;
         float t[7];
 #pragma unroll
         for (int q = 0; q < 7; q++) t[q] = src[(q * K + k) * kRepBlock + lane];
@@ -160,7 +167,8 @@ __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P
         mbar_init(&stall_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == helper && total > 0) make_pre(0);
+    make_window(0);
+    make_window(1);
     __syncthreads();
     if (total > 0) {
         pair_of(0, ci0, cj0);
@@ -175,7 +183,9 @@ __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P
 
     bool aborted = false;
     for (int m = 0; m < total; m++) {
-        if (warp == helper && m + 1 < total) make_pre(m + 1);
+        // window w+1 during the first move of window w (its buffer's last
+        // reader is behind barrier kWinK*w - 1)
+        if (m >= kWinK && m % kWinK == 0) make_window(m / kWinK + 1);
         // ---- field pass m
         float hix[K], hiy[K], hjx[K], hjy[K];
 #pragma unroll
