@@ -139,8 +139,7 @@ struct SampleHost {
     int64_t site_entries = 0;
     double exec_flops_lists = 0.0;   // FP32 ops per replica to accumulate all N site lists once
     int64_t g4_off = -1;             // dense: into d_g4re / d_mask
-    int fc_tiles = 0;                // site lists are fully connected tiles
-    int flat_groups = 0;             // every group of the site lists has one data entry
+    int fc_tiles = 0;                // site lists are fully connected tiles (else group records)
     int64_t nq_dense = 0;
 };
 
@@ -881,12 +880,11 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
             std::vector<uint8_t>().swap(maskh[k]);
         }
         h.fc_tiles = fc ? 1 : 0;
-        if (!fc) build_site_lists(N, h.g2re.data(), h.h2_active, qsv[k], lists[k]);
-        h.flat_groups = (!fc && lists_single_groups(lists[k])) ? 1 : 0;
+        if (!fc) build_site_lists(N, h.g2re.data(), h.h2_active, qsv[k], lists[k], true);
         build_q64(qsv[k], q64[k]);
         std::vector<QuartetRec>().swap(qsv[k]);
         h.site_entries = (int64_t)lists[k].entries.size();
-        h.exec_flops_lists = list_exec_flops(lists[k], N, fc);
+        h.exec_flops_lists = list_exec_flops(lists[k], N, fc, !fc);
     }
 
     const auto t_p3 = clk();
@@ -902,7 +900,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         d.h2_active = h.h2_active;
         d.variant = variant;
         d.fc_tiles = h.fc_tiles;
-        d.flat_groups = h.flat_groups;
+        d.pad0 = 0;
         d.spin_off = spin_off;
         d.rep_off = rep_off;
         d.split_off = split_total;

@@ -8,12 +8,18 @@
 //   per-replica arrays [sum_s R_s]          energy (f64), accepted/proposed
 //                                           (i64), beta (f64), RNG key (u64),
 //                                           constraint target (f64)
-//   site lists int2   [sum_s entries_s]     per sample, per site: groups of one
-//                                           header {len, p<<16|o1} followed by
-//                                           len data {g (f32 bits), o2}, packed
+//   site lists int2   [sum_s entries_s]     per sample, per site: groups of
+//                                           terms with the same (p, o1), one
+//                                           16-byte record {g (f32 bits), o2,
+//                                           p<<16|o1, last} per term (or the
+//                                           fully connected tiles below), packed
 //                                           in TMA chunks of <= 256 entries that
 //                                           hold whole groups, start 16-byte
-//                                           aligned and have an even length
+//                                           aligned and have an even length.
+//                                           The pair sub-lists of the two-pass
+//                                           sweep keep the group format: a
+//                                           header {len, p<<16|o1} and len data
+//                                           entries {g, o2}
 //   chunk starts int64 [n_chunks + 1]       entry offset of every chunk
 //   site chunks int32 [sum_s N_s * 33]      first chunk of each of the 32
 //                                           balanced parts of a site's list
@@ -66,8 +72,8 @@ struct SampleDev {
     int R;                 // replicas of this sample
     int h2_active;
     int variant;           // 0 sphere (dense), 1 smoothed cube (sparse)
-    int fc_tiles;          // 1: site lists are fully connected tiles (see below)
-    int flat_groups;       // 1: every group has one data entry (16-byte records)
+    int fc_tiles;          // 1: site lists are fully connected tiles (see below), 0: group records
+    int pad0;
     int64_t spin_off;      // float2 index of site 0, replica 0
     int64_t rep_off;       // index into the per-replica arrays
     int64_t split_off;     // index into site chunks (N*33 entries)

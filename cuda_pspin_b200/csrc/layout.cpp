@@ -82,9 +82,12 @@ static void pack_site(const std::vector<int2>& site, const std::vector<std::pair
 }
 
 // Sorts one list's records by (p, o1, o2), cuts groups of equal (p, o1) at
-// kGroupMax data entries and packs them as list `id`.
+// kGroupMax data entries and packs them as list `id`: as a header and data
+// entries, or (records) as one 16-byte record {g, o2, p<<16|o1, last} per
+// data entry, `last` marking the group's final record.
 static void group_and_pack(std::vector<Rec>& v, int id, std::vector<int2>& site,
-                           std::vector<std::pair<int64_t, int64_t>>& groups, SiteLists& out, int stride = 1) {
+                           std::vector<std::pair<int64_t, int64_t>>& groups, SiteLists& out, int stride = 1,
+                           bool records = false) {
     std::sort(v.begin(), v.end(), [](const Rec& a, const Rec& b) {
         return a.key != b.key ? a.key < b.key : a.o2 < b.o2;
     });
@@ -95,11 +98,12 @@ static void group_and_pack(std::vector<Rec>& v, int id, std::vector<int2>& site,
         size_t e = t;
         while (e < v.size() && v[e].key == v[t].key && (int)(e - t) < kGroupMax) e++;
         const int64_t gb = (int64_t)site.size();
-        site.push_back(make_int2((int)(e - t), v[t].key));
+        if (!records) site.push_back(make_int2((int)(e - t), v[t].key));
         for (size_t u = t; u < e; u++) {
             int bits;
             std::memcpy(&bits, &v[u].g, sizeof(int));
             site.push_back(make_int2(bits, v[u].o2));
+            if (records) site.push_back(make_int2(v[t].key, u + 1 == e ? 1 : 0));
         }
         groups.push_back({gb, (int64_t)site.size()});
         t = e;
@@ -145,7 +149,7 @@ void build_pair_lists(int N, const double* g2re, int h2_active, const std::vecto
 }
 
 void build_site_lists(int N, const double* g2re, int h2_active, const std::vector<QuartetRec>& qs,
-                      SiteLists& out) {
+                      SiteLists& out, bool records) {
     std::vector<std::vector<Rec>> per(N);
     std::vector<int64_t> cnt(N, 0);
     for (const QuartetRec& r : qs) { cnt[r.i]++; cnt[r.j]++; cnt[r.k]++; cnt[r.l]++; }
@@ -174,7 +178,7 @@ void build_site_lists(int N, const double* g2re, int h2_active, const std::vecto
     out.site_chunks.assign((size_t)N * (kSplit + 1), 0);
     std::vector<std::pair<int64_t, int64_t>> groups;   // [begin, end) in a site-local list
     std::vector<int2> site;
-    for (int m = 0; m < N; m++) group_and_pack(per[m], m, site, groups, out);
+    for (int m = 0; m < N; m++) group_and_pack(per[m], m, site, groups, out, 1, records);
 }
 
 static inline int64_t encode_sorted(int a, int b, int c, int d) {
@@ -254,7 +258,7 @@ void build_site_tiles_fc(int N, const double* g2re, int h2_active, const double*
 // (a_p conj(a_o1): 2 FMA + 2 MUL; the field update: 4 FMA) and 4 per data
 // entry (2 FMA); a fully connected tile costs 56 per header (4 partners x 14)
 // and 16 per row (8 FMA: 4 couplings times one gathered amplitude).
-double list_exec_flops(const SiteLists& L, int N, bool tiles) {
+double list_exec_flops(const SiteLists& L, int N, bool tiles, bool records) {
     double total = 0.0;
     const int64_t nchunks = (int64_t)L.chunk_start.size();
     for (int m = 0; m < N; m++) {
@@ -271,6 +275,8 @@ double list_exec_flops(const SiteLists& L, int N, bool tiles) {
                     total += 56.0 + 16.0 * (hi - lo);
                     u += 1 + (hi - lo);
                 }
+            } else if (records) {
+                for (int64_t u = 0; u + 1 < n; u += 2) total += 4.0 + (R[u + 1].y ? 14.0 : 0.0);
             } else {
                 for (int64_t u = 0; u < n;) {
                     const int len = R[u].x;
@@ -281,17 +287,6 @@ double list_exec_flops(const SiteLists& L, int N, bool tiles) {
         }
     }
     return total;
-}
-
-bool lists_single_groups(const SiteLists& L) {
-    const int64_t nchunks = (int64_t)L.chunk_start.size();
-    for (int64_t c = 0; c < nchunks; c++) {
-        const int64_t b = L.chunk_start[c];
-        const int64_t e = (c + 1 < nchunks) ? L.chunk_start[c + 1] : (int64_t)L.entries.size();
-        for (int64_t u = b; u < e; u += 2)
-            if (L.entries[u].x != 1) return false;
-    }
-    return true;
 }
 
 void build_q64(const std::vector<QuartetRec>& qs, std::vector<Q64>& out) {

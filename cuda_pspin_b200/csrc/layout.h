@@ -18,8 +18,12 @@ struct SiteLists {
     std::vector<int> site_chunks;      // N*(kSplit+1) sample-relative chunk indices
 };
 
+// Per-site lists in the group format, or (records) as 16-byte records
+// {g, o2, p<<16|o1, last}: the same groups, one record per data entry, so a
+// record's position never depends on an earlier header and the loads of
+// consecutive records overlap; the sweep kernels read site lists this way.
 void build_site_lists(int N, const double* g2re, int h2_active, const std::vector<QuartetRec>& qs,
-                      SiteLists& out);
+                      SiteLists& out, bool records = false);
 // Sub-lists of the terms that couple the two sites of a pair (same group
 // format): for i < j and P = j(j-1)/2 + i, list 2P holds site i's terms that
 // contain a_j, list 2P+1 site j's terms that contain a_i.  Each term of a
@@ -29,15 +33,13 @@ void build_pair_lists(int N, const double* g2re, int h2_active, const std::vecto
 // fully connected tiles from the dense g4 (channel 0 everywhere) and g2
 void build_site_tiles_fc(int N, const double* g2re, int h2_active, const double* g4re, SiteLists& out);
 void build_q64(const std::vector<QuartetRec>& qs, std::vector<Q64>& out);
-// true when every group of the lists has exactly one data entry (sparse
-// samples, as a rule): the lists are then a flat array of 16-byte records
-// {1, p<<16|o1, g, o2} with no padding entries
-bool lists_single_groups(const SiteLists& L);
+
 // FP32 operations the sweep kernels execute, per replica, to accumulate the
 // lists of all N sites once (the expected work of one sweep's N/2 moves over
 // their two sites each), walking the packed chunks exactly as
-// accumulate_chunk / accumulate_tiles do (padding words included).
-double list_exec_flops(const SiteLists& L, int N, bool tiles);
+// accumulate_chunk / accumulate_records / accumulate_tiles do (padding
+// words included).
+double list_exec_flops(const SiteLists& L, int N, bool tiles, bool records = false);
 // every active (q, ch) of a dense mask in q order
 void dense_quartets(int N, const double* g4re, const uint8_t* mask, std::vector<QuartetRec>& out);
 

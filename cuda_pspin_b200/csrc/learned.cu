@@ -278,9 +278,10 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
                 if (!ok_wait) break;               // stop consuming and issuing; abort in reduce()
                 const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
                 const int k2 = 2 * (which & 1);
-                if (S.fc_tiles && which < 2)       // unrolled by 2: the kernel is held to 80 registers
+                if (which >= 2) accumulate_chunk(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
+                else if (S.fc_tiles)               // unrolled by 2: the kernel is held to 80 registers
                     accumulate_tiles<2>(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
-                else accumulate_chunk(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
+                else accumulate_records<2>(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
                 consumed++;
                 __syncwarp();
                 if (lane == 0) fence_async_shared();

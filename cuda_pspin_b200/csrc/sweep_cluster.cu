@@ -212,10 +212,10 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
             if (!ok) break;                        // stop consuming and issuing; abort below
             if (tg.x & 1) {
                 if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
-                else accumulate_chunk(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
+                else accumulate_records(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
             } else {
                 if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
-                else accumulate_chunk(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
+                else accumulate_records(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
             }
             consumed++;
             __syncwarp();

@@ -286,30 +286,36 @@ __device__ __forceinline__ void accumulate_chunk(const int2* __restrict__ R, int
     }
 }
 
-// The same for lists whose groups all have one data entry, read as 16-byte
-// records {1, p<<16|o1, g, o2} with no dependence of one record's position
-// on the previous header, so the records' loads overlap.  The arithmetic is
-// accumulate_chunk's for a group of one entry, so the result is bit for bit
-// the same.
+// The same groups stored as 16-byte records {g, o2, p<<16|o1, last}, one
+// per data entry: a record's position does not depend on an earlier header,
+// so the loads of consecutive records overlap.  The arithmetic is
+// accumulate_chunk's, operation for operation: Y accumulates the group's
+// entries in order from zero and h takes a_p conj(a_o1) Y at the group's
+// last record.
 template <int kUnroll = 4>
-__device__ __forceinline__ void accumulate_flat(const int2* __restrict__ R2, int n,
-                                                const float2* __restrict__ sp, int lane,
-                                                float& hx, float& hy) {
+__device__ __forceinline__ void accumulate_records(const int2* __restrict__ R2, int n,
+                                                   const float2* __restrict__ sp, int lane,
+                                                   float& hx, float& hy) {
     const int4* __restrict__ R = reinterpret_cast<const int4*>(R2);
     const int nr = n >> 1;
+    float yx = 0.f, yy = 0.f;
 #pragma unroll kUnroll
     for (int r = 0; r < nr; r++) {
         const int4 q = R[r];
-        const int p = q.y >> 16, o1 = q.y & 0xFFFF;
-        const float2 ap = sp[p * kRepBlock + lane];
-        const float2 ao = sp[o1 * kRepBlock + lane];
-        const float2 a = sp[q.w * kRepBlock + lane];
-        const float g = __int_as_float(q.z);
-        const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
-        const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
-        const float yx = fmaf(g, a.x, 0.f), yy = fmaf(-g, a.y, 0.f);
-        hx = fmaf(px, yx, fmaf(-py, yy, hx));
-        hy = fmaf(px, yy, fmaf(py, yx, hy));
+        const float g = __int_as_float(q.x);
+        const float2 a = sp[q.y * kRepBlock + lane];
+        yx = fmaf(g, a.x, yx);           // Y += g conj(a_o2)
+        yy = fmaf(-g, a.y, yy);
+        if (q.w) {
+            const float2 ap = sp[(q.z >> 16) * kRepBlock + lane];
+            const float2 ao = sp[(q.z & 0xFFFF) * kRepBlock + lane];
+            const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
+            const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
+            hx = fmaf(px, yx, fmaf(-py, yy, hx));
+            hy = fmaf(px, yy, fmaf(py, yx, hy));
+            yx = 0.f;
+            yy = 0.f;
+        }
     }
 }
 
@@ -361,44 +367,8 @@ __device__ __forceinline__ void accumulate_tiles(const int2* __restrict__ R2, in
 // The same accumulations for a block of 32K replicas stored [site][K][32]
 // (replica k*32 + lane of the block at sp[(site*K + k)*32 + lane]): each
 // staged coupling is read once and used for the lane's K replicas.  The
-// summation order per replica is that of accumulate_chunk / accumulate_tiles.
-template <int K>
-__device__ __forceinline__ void accumulate_chunk_k(const int2* __restrict__ R, int n,
-                                                   const float2* __restrict__ sp, int lane,
-                                                   float (&hx)[K], float (&hy)[K]) {
-    int e = 0;
-    while (e < n) {
-        const int2 h = R[e];
-        const int len = h.x;
-        const int p = h.y >> 16, o1 = h.y & 0xFFFF;
-        float yx[K], yy[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) yx[k] = yy[k] = 0.f;
-        const int2* __restrict__ d = R + e + 1;
-#pragma unroll 4
-        for (int t = 0; t < len; t++) {
-            const int2 v = d[t];
-            const float g = __int_as_float(v.x);
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                const float2 a = sp[(v.y * K + k) * kRepBlock + lane];
-                yx[k] = fmaf(g, a.x, yx[k]);
-                yy[k] = fmaf(-g, a.y, yy[k]);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            const float2 ap = sp[(p * K + k) * kRepBlock + lane];
-            const float2 ao = sp[(o1 * K + k) * kRepBlock + lane];
-            const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
-            const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
-            hx[k] = fmaf(px, yx[k], fmaf(-py, yy[k], hx[k]));
-            hy[k] = fmaf(px, yy[k], fmaf(py, yx[k], hy[k]));
-        }
-        e += len + 1;
-    }
-}
-
+// summation order per replica is that of accumulate_tiles /
+// accumulate_records.
 template <int K, int kUnroll>
 __device__ __forceinline__ void accumulate_tiles_k(const int2* __restrict__ R2, int n,
                                                    const float2* __restrict__ sp, int lane,
@@ -443,6 +413,42 @@ __device__ __forceinline__ void accumulate_tiles_k(const int2* __restrict__ R2, 
             }
         }
         e += 1 + len;
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void accumulate_records_k(const int2* __restrict__ R2, int n,
+                                                     const float2* __restrict__ sp, int lane,
+                                                     float (&hx)[K], float (&hy)[K]) {
+    const int4* __restrict__ R = reinterpret_cast<const int4*>(R2);
+    const int nr = n >> 1;
+    float yx[K], yy[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) yx[k] = yy[k] = 0.f;
+#pragma unroll 4
+    for (int r = 0; r < nr; r++) {
+        const int4 q = R[r];
+        const float g = __int_as_float(q.x);
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const float2 a = sp[(q.y * K + k) * kRepBlock + lane];
+            yx[k] = fmaf(g, a.x, yx[k]);
+            yy[k] = fmaf(-g, a.y, yy[k]);
+        }
+        if (q.w) {
+            const int p = q.z >> 16, o1 = q.z & 0xFFFF;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const float2 ap = sp[(p * K + k) * kRepBlock + lane];
+                const float2 ao = sp[(o1 * K + k) * kRepBlock + lane];
+                const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
+                const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
+                hx[k] = fmaf(px, yx[k], fmaf(-py, yy[k], hx[k]));
+                hy[k] = fmaf(px, yy[k], fmaf(py, yx[k], hy[k]));
+                yx[k] = 0.f;
+                yy[k] = 0.f;
+            }
+        }
     }
 }
 

@@ -202,10 +202,10 @@ __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P
             if (!ok) break;
             if ((tg.x & 1) == 0) {
                 if (S.fc_tiles) accumulate_tiles_k<K, 4>(ring + slot * kStage, tg.y, sp, lane, hix, hiy);
-                else accumulate_chunk_k<K>(ring + slot * kStage, tg.y, sp, lane, hix, hiy);
+                else accumulate_records_k<K>(ring + slot * kStage, tg.y, sp, lane, hix, hiy);
             } else {
                 if (S.fc_tiles) accumulate_tiles_k<K, 4>(ring + slot * kStage, tg.y, sp, lane, hjx, hjy);
-                else accumulate_chunk_k<K>(ring + slot * kStage, tg.y, sp, lane, hjx, hjy);
+                else accumulate_records_k<K>(ring + slot * kStage, tg.y, sp, lane, hjx, hjy);
             }
             consumed++;
             __syncwarp();

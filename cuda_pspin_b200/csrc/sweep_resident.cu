@@ -218,12 +218,9 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
                 if (S.fc_tiles) {
                     accumulate_tiles(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
                     accumulate_tiles(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
-                } else if (S.flat_groups) {
-                    accumulate_flat(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
-                    accumulate_flat(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
                 } else {
-                    accumulate_chunk(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
-                    accumulate_chunk(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
+                    accumulate_records(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
+                    accumulate_records(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
                 }
                 const float dix = ain.x - ai.x, diy = ain.y - ai.y;
                 const float djx = ajn.x - aj.x, djy = ajn.y - aj.y;
