@@ -54,9 +54,6 @@ inline size_t cluster_smem_bytes(int N, int warps, int C) {
     return cluster_buffer_offset(N, warps) + (size_t)2 * C * warps * kRepBlock * sizeof(float4) + 16 + kStaticSmem;
 }
 
-__device__ __forceinline__ void add4(float4& a, const float4 b) {
-    a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
-}
 
 template <int VARIANT>
 __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams P) {
@@ -246,13 +243,7 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
         }
 
         // ---- decision m, the same in every warp
-        float4 hs = buf[lane];
-        for (int w = 1; w < W; w++) add4(hs, buf[w * kRepBlock + lane]);
-        for (int q = 1; q < C; q++) {
-            float4 part = buf[(q * W) * kRepBlock + lane];
-            for (int w = 1; w < W; w++) add4(part, buf[(q * W + w) * kRepBlock + lane]);
-            add4(hs, part);
-        }
+        const float4 hs = sum_partials(buf + lane, C, W, kRepBlock);
         const float dix = cain.x - cai.x, diy = cain.y - cai.y;
         const float djx = cajn.x - caj.x, djy = cajn.y - caj.y;
         const float dE = -fmaf(dix, hs.x, -diy * hs.y) - fmaf(djx, hs.z, -djy * hs.w);

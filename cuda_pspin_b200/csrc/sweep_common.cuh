@@ -287,11 +287,28 @@ __device__ __forceinline__ void accumulate_chunk(const int2* __restrict__ R, int
 }
 
 // The same groups stored as 16-byte records {g, o2, p<<16|o1, last}, one
-// per data entry: a record's position does not depend on an earlier header,
-// so the loads of consecutive records overlap.  The arithmetic is
-// accumulate_chunk's, operation for operation: Y accumulates the group's
-// entries in order from zero and h takes a_p conj(a_o1) Y at the group's
-// last record.
+// per data entry: a record's position does not depend on an earlier header.
+// Records are taken four at a time with every shared-memory load of the
+// four (records, then a_o2, a_p, a_o1 of each) issued before the arithmetic,
+// so a batch costs about two load latencies instead of two per record.  The
+// arithmetic is accumulate_chunk's, operation for operation: Y accumulates
+// the group's entries in order from zero and h takes a_p conj(a_o1) Y at the
+// group's last record.
+__device__ __forceinline__ void record_step(const int4 q, const float2 a, const float2 ap, const float2 ao,
+                                            float& yx, float& yy, float& hx, float& hy) {
+    const float g = __int_as_float(q.x);
+    yx = fmaf(g, a.x, yx);               // Y += g conj(a_o2)
+    yy = fmaf(-g, a.y, yy);
+    if (q.w) {
+        const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
+        const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
+        hx = fmaf(px, yx, fmaf(-py, yy, hx));
+        hy = fmaf(px, yy, fmaf(py, yx, hy));
+        yx = 0.f;
+        yy = 0.f;
+    }
+}
+
 template <int kUnroll = 4>
 __device__ __forceinline__ void accumulate_records(const int2* __restrict__ R2, int n,
                                                    const float2* __restrict__ sp, int lane,
@@ -299,23 +316,25 @@ __device__ __forceinline__ void accumulate_records(const int2* __restrict__ R2, 
     const int4* __restrict__ R = reinterpret_cast<const int4*>(R2);
     const int nr = n >> 1;
     float yx = 0.f, yy = 0.f;
-#pragma unroll kUnroll
-    for (int r = 0; r < nr; r++) {
-        const int4 q = R[r];
-        const float g = __int_as_float(q.x);
-        const float2 a = sp[q.y * kRepBlock + lane];
-        yx = fmaf(g, a.x, yx);           // Y += g conj(a_o2)
-        yy = fmaf(-g, a.y, yy);
-        if (q.w) {
-            const float2 ap = sp[(q.z >> 16) * kRepBlock + lane];
-            const float2 ao = sp[(q.z & 0xFFFF) * kRepBlock + lane];
-            const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
-            const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
-            hx = fmaf(px, yx, fmaf(-py, yy, hx));
-            hy = fmaf(px, yy, fmaf(py, yx, hy));
-            yx = 0.f;
-            yy = 0.f;
+    int r = 0;
+    for (; r + kUnroll <= nr; r += kUnroll) {
+        int4 q[kUnroll];
+        float2 a[kUnroll], ap[kUnroll], ao[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) q[u] = R[r + u];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            a[u] = sp[q[u].y * kRepBlock + lane];
+            ap[u] = sp[(q[u].z >> 16) * kRepBlock + lane];
+            ao[u] = sp[(q[u].z & 0xFFFF) * kRepBlock + lane];
         }
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) record_step(q[u], a[u], ap[u], ao[u], yx, yy, hx, hy);
+    }
+    for (; r < nr; r++) {
+        const int4 q = R[r];
+        record_step(q, sp[q.y * kRepBlock + lane], sp[(q.z >> 16) * kRepBlock + lane],
+                    sp[(q.z & 0xFFFF) * kRepBlock + lane], yx, yy, hx, hy);
     }
 }
 
@@ -425,31 +444,63 @@ __device__ __forceinline__ void accumulate_records_k(const int2* __restrict__ R2
     float yx[K], yy[K];
 #pragma unroll
     for (int k = 0; k < K; k++) yx[k] = yy[k] = 0.f;
-#pragma unroll 4
-    for (int r = 0; r < nr; r++) {
-        const int4 q = R[r];
-        const float g = __int_as_float(q.x);
+    constexpr int kB = 2;                // records per batch (K amplitudes each)
+    int r = 0;
+    for (; r + kB <= nr; r += kB) {
+        int4 q[kB];
+        float2 a[kB][K], ap[kB][K], ao[kB][K];
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            const float2 a = sp[(q.y * K + k) * kRepBlock + lane];
-            yx[k] = fmaf(g, a.x, yx[k]);
-            yy[k] = fmaf(-g, a.y, yy[k]);
-        }
-        if (q.w) {
-            const int p = q.z >> 16, o1 = q.z & 0xFFFF;
+        for (int u = 0; u < kB; u++) q[u] = R[r + u];
+#pragma unroll
+        for (int u = 0; u < kB; u++)
 #pragma unroll
             for (int k = 0; k < K; k++) {
-                const float2 ap = sp[(p * K + k) * kRepBlock + lane];
-                const float2 ao = sp[(o1 * K + k) * kRepBlock + lane];
-                const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
-                const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
-                hx[k] = fmaf(px, yx[k], fmaf(-py, yy[k], hx[k]));
-                hy[k] = fmaf(px, yy[k], fmaf(py, yx[k], hy[k]));
-                yx[k] = 0.f;
-                yy[k] = 0.f;
+                a[u][k] = sp[(q[u].y * K + k) * kRepBlock + lane];
+                ap[u][k] = sp[((q[u].z >> 16) * K + k) * kRepBlock + lane];
+                ao[u][k] = sp[((q[u].z & 0xFFFF) * K + k) * kRepBlock + lane];
             }
-        }
+#pragma unroll
+        for (int u = 0; u < kB; u++)
+#pragma unroll
+            for (int k = 0; k < K; k++) record_step(q[u], a[u][k], ap[u][k], ao[u][k], yx[k], yy[k], hx[k], hy[k]);
     }
+    for (; r < nr; r++) {
+        const int4 q = R[r];
+#pragma unroll
+        for (int k = 0; k < K; k++)
+            record_step(q, sp[(q.y * K + k) * kRepBlock + lane], sp[((q.z >> 16) * K + k) * kRepBlock + lane],
+                        sp[((q.z & 0xFFFF) * K + k) * kRepBlock + lane], yx[k], yy[k], hx[k], hy[k]);
+    }
+}
+
+// The field partials of the C CTAs x W warps of a block, summed in the fixed
+// order the cluster kernels use -- each CTA's warps in order, then the CTAs
+// in rank order -- from slots buf[(q*W + w) * stride], with the loads of
+// four slots in flight before their additions (the same additions in the
+// same order as one load per addition).
+__device__ __forceinline__ void add4v(float4& a, const float4 b) {
+    a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
+}
+__device__ __forceinline__ float4 sum_partials(const float4* buf, int C, int W, int stride) {
+    float4 hs = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int q = 0; q < C; q++) {
+        float4 part = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int w0 = 0; w0 < W; w0 += 4) {
+            float4 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (w0 + u < W) v[u] = buf[(size_t)(q * W + w0 + u) * stride];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (w0 + u < W) {
+                    if (w0 + u == 0) part = v[u];
+                    else add4v(part, v[u]);
+                }
+        }
+        if (q == 0) hs = part;
+        else add4v(hs, part);
+    }
+    return hs;
 }
 
 // ---------------------------------------------------------------- clusters

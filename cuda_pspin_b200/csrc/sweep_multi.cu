@@ -34,9 +34,6 @@ inline size_t multi_smem_bytes(int N, int W, int C, int K) {   // + the static r
     return multi_buffer_offset(N, W, K) + (size_t)2 * C * W * K * kRepBlock * sizeof(float4) + 16 + kStaticSmem;
 }
 
-__device__ __forceinline__ void add4m(float4& a, const float4 b) {
-    a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
-}
 
 template <int VARIANT, int K>
 __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P) {
@@ -252,13 +249,7 @@ __global__ void __launch_bounds__(256, 1) sweep_multi_kernel(const SweepParams P
         float2 ai_post[K], aj_post[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            float4 hs = buf[(size_t)k * kRepBlock + lane];
-            for (int w = 1; w < W; w++) add4m(hs, buf[(size_t)(w * K + k) * kRepBlock + lane]);
-            for (int q = 1; q < C; q++) {
-                float4 part = buf[(size_t)(q * W * K + k) * kRepBlock + lane];
-                for (int w = 1; w < W; w++) add4m(part, buf[(size_t)((q * W + w) * K + k) * kRepBlock + lane]);
-                add4m(hs, part);
-            }
+            const float4 hs = sum_partials(buf + (size_t)k * kRepBlock + lane, C, W, K * kRepBlock);
             const float dix = cain[k].x - cai[k].x, diy = cain[k].y - cai[k].y;
             const float djx = cajn[k].x - caj[k].x, djy = cajn[k].y - caj[k].y;
             const float dE = -fmaf(dix, hs.x, -diy * hs.y) - fmaf(djx, hs.z, -djy * hs.w);
