@@ -140,6 +140,7 @@ struct SampleHost {
     double exec_flops_lists = 0.0;   // FP32 ops per replica to accumulate all N site lists once
     int64_t g4_off = -1;             // dense: into d_g4re / d_mask
     int fc_tiles = 0;                // site lists are fully connected tiles (else group records)
+    int single_groups = 0;           // group records, every group of one entry
     int64_t nq_dense = 0;
 };
 
@@ -881,6 +882,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         }
         h.fc_tiles = fc ? 1 : 0;
         if (!fc) build_site_lists(N, h.g2re.data(), h.h2_active, qsv[k], lists[k], true);
+        h.single_groups = (!fc && records_single_groups(lists[k])) ? 1 : 0;
         build_q64(qsv[k], q64[k]);
         std::vector<QuartetRec>().swap(qsv[k]);
         h.site_entries = (int64_t)lists[k].entries.size();
@@ -900,7 +902,7 @@ extern "C" int pspin_create_batch(const pspin_config* cfgs, int n, int variant, 
         d.h2_active = h.h2_active;
         d.variant = variant;
         d.fc_tiles = h.fc_tiles;
-        d.pad0 = 0;
+        d.single_groups = h.single_groups;
         d.spin_off = spin_off;
         d.rep_off = rep_off;
         d.split_off = split_total;

@@ -73,7 +73,7 @@ struct SampleDev {
     int h2_active;
     int variant;           // 0 sphere (dense), 1 smoothed cube (sparse)
     int fc_tiles;          // 1: site lists are fully connected tiles (see below), 0: group records
-    int pad0;
+    int single_groups;     // group records only, every group of one entry (each record ends its group)
     int64_t spin_off;      // float2 index of site 0, replica 0
     int64_t rep_off;       // index into the per-replica arrays
     int64_t split_off;     // index into site chunks (N*33 entries)

@@ -289,6 +289,12 @@ double list_exec_flops(const SiteLists& L, int N, bool tiles, bool records) {
     return total;
 }
 
+bool records_single_groups(const SiteLists& L) {
+    for (size_t u = 0; u + 1 < L.entries.size(); u += 2)
+        if (L.entries[u + 1].y != 1) return false;
+    return true;
+}
+
 void build_q64(const std::vector<QuartetRec>& qs, std::vector<Q64>& out) {
     out.resize(qs.size());
     for (size_t t = 0; t < qs.size(); t++) {

@@ -33,6 +33,8 @@ void build_pair_lists(int N, const double* g2re, int h2_active, const std::vecto
 // fully connected tiles from the dense g4 (channel 0 everywhere) and g2
 void build_site_tiles_fc(int N, const double* g2re, int h2_active, const double* g4re, SiteLists& out);
 void build_q64(const std::vector<QuartetRec>& qs, std::vector<Q64>& out);
+// site lists in the record format: does every record end its group?
+bool records_single_groups(const SiteLists& L);
 
 // FP32 operations the sweep kernels execute, per replica, to accumulate the
 // lists of all N sites once (the expected work of one sweep's N/2 moves over

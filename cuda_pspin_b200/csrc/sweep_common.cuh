@@ -288,18 +288,21 @@ __device__ __forceinline__ void accumulate_chunk(const int2* __restrict__ R, int
 
 // The same groups stored as 16-byte records {g, o2, p<<16|o1, last}, one
 // per data entry: a record's position does not depend on an earlier header.
-// Records are taken four at a time with every shared-memory load of the
-// four (records, then a_o2, a_p, a_o1 of each) issued before the arithmetic,
-// so a batch costs about two load latencies instead of two per record.  The
-// arithmetic is accumulate_chunk's, operation for operation: Y accumulates
-// the group's entries in order from zero and h takes a_p conj(a_o1) Y at the
-// group's last record.
+// Records are taken kUnroll at a time with their shared-memory loads (the
+// records, then each a_o2, and a_p, a_o1 where the record ends a group --
+// predicated, so no other record reads them) issued before the arithmetic,
+// so a batch costs about two load latencies.  The arithmetic is
+// accumulate_chunk's, operation for operation: Y accumulates the group's
+// entries in order from zero and h takes a_p conj(a_o1) Y at the group's
+// last record.  kSingle: every record ends its group (groups of one entry,
+// the rule for sparse samples), so the test is compiled out.
+template <bool kSingle>
 __device__ __forceinline__ void record_step(const int4 q, const float2 a, const float2 ap, const float2 ao,
                                             float& yx, float& yy, float& hx, float& hy) {
     const float g = __int_as_float(q.x);
     yx = fmaf(g, a.x, yx);               // Y += g conj(a_o2)
     yy = fmaf(-g, a.y, yy);
-    if (q.w) {
+    if (kSingle || q.w) {
         const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
         const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
         hx = fmaf(px, yx, fmaf(-py, yy, hx));
@@ -309,7 +312,7 @@ __device__ __forceinline__ void record_step(const int4 q, const float2 a, const 
     }
 }
 
-template <int kUnroll = 4>
+template <int kUnroll = 4, bool kSingle = false>
 __device__ __forceinline__ void accumulate_records(const int2* __restrict__ R2, int n,
                                                    const float2* __restrict__ sp, int lane,
                                                    float& hx, float& hy) {
@@ -325,16 +328,19 @@ __device__ __forceinline__ void accumulate_records(const int2* __restrict__ R2, 
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) {
             a[u] = sp[q[u].y * kRepBlock + lane];
-            ap[u] = sp[(q[u].z >> 16) * kRepBlock + lane];
-            ao[u] = sp[(q[u].z & 0xFFFF) * kRepBlock + lane];
+            ap[u] = ao[u] = make_float2(0.f, 0.f);
+            if (kSingle || q[u].w) {
+                ap[u] = sp[(q[u].z >> 16) * kRepBlock + lane];
+                ao[u] = sp[(q[u].z & 0xFFFF) * kRepBlock + lane];
+            }
         }
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++) record_step(q[u], a[u], ap[u], ao[u], yx, yy, hx, hy);
+        for (int u = 0; u < kUnroll; u++) record_step<kSingle>(q[u], a[u], ap[u], ao[u], yx, yy, hx, hy);
     }
     for (; r < nr; r++) {
         const int4 q = R[r];
-        record_step(q, sp[q.y * kRepBlock + lane], sp[(q.z >> 16) * kRepBlock + lane],
-                    sp[(q.z & 0xFFFF) * kRepBlock + lane], yx, yy, hx, hy);
+        record_step<kSingle>(q, sp[q.y * kRepBlock + lane], sp[(q.z >> 16) * kRepBlock + lane],
+                             sp[(q.z & 0xFFFF) * kRepBlock + lane], yx, yy, hx, hy);
     }
 }
 
@@ -456,20 +462,24 @@ __device__ __forceinline__ void accumulate_records_k(const int2* __restrict__ R2
 #pragma unroll
             for (int k = 0; k < K; k++) {
                 a[u][k] = sp[(q[u].y * K + k) * kRepBlock + lane];
-                ap[u][k] = sp[((q[u].z >> 16) * K + k) * kRepBlock + lane];
-                ao[u][k] = sp[((q[u].z & 0xFFFF) * K + k) * kRepBlock + lane];
+                ap[u][k] = ao[u][k] = make_float2(0.f, 0.f);
+                if (q[u].w) {
+                    ap[u][k] = sp[((q[u].z >> 16) * K + k) * kRepBlock + lane];
+                    ao[u][k] = sp[((q[u].z & 0xFFFF) * K + k) * kRepBlock + lane];
+                }
             }
 #pragma unroll
         for (int u = 0; u < kB; u++)
 #pragma unroll
-            for (int k = 0; k < K; k++) record_step(q[u], a[u][k], ap[u][k], ao[u][k], yx[k], yy[k], hx[k], hy[k]);
+            for (int k = 0; k < K; k++)
+                record_step<false>(q[u], a[u][k], ap[u][k], ao[u][k], yx[k], yy[k], hx[k], hy[k]);
     }
     for (; r < nr; r++) {
         const int4 q = R[r];
 #pragma unroll
         for (int k = 0; k < K; k++)
-            record_step(q, sp[(q.y * K + k) * kRepBlock + lane], sp[((q.z >> 16) * K + k) * kRepBlock + lane],
-                        sp[((q.z & 0xFFFF) * K + k) * kRepBlock + lane], yx[k], yy[k], hx[k], hy[k]);
+            record_step<false>(q, sp[(q.y * K + k) * kRepBlock + lane], sp[((q.z >> 16) * K + k) * kRepBlock + lane],
+                               sp[((q.z & 0xFFFF) * K + k) * kRepBlock + lane], yx[k], yy[k], hx[k], hy[k]);
     }
 }
 

@@ -218,6 +218,9 @@ __global__ void __launch_bounds__(256) sweep_resident_kernel(const SweepParams P
                 if (S.fc_tiles) {
                     accumulate_tiles(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
                     accumulate_tiles(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
+                } else if (S.single_groups) {
+                    accumulate_records<4, true>(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
+                    accumulate_records<4, true>(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
                 } else {
                     accumulate_records(L + ri.x, ri.y - ri.x, sp, lane, hix, hiy);
                     accumulate_records(L + rj.x, rj.y - rj.x, sp, lane, hjx, hjy);
