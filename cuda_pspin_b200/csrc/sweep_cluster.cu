@@ -55,7 +55,12 @@ inline size_t cluster_smem_bytes(int N, int warps, int C) {
 }
 
 
-template <int VARIANT>
+// kBatch: the group records are read in batches whose loads are all in
+// flight before their arithmetic (few blocks, so each warp waits on its own
+// chain's latency); otherwise one record at a time, loading a_p, a_o1 once
+// per group (many blocks share the SMs; fewer shared-memory loads and no
+// register spill at 128 registers).
+template <int VARIANT, bool kBatch>
 __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int C = P.cluster;
@@ -209,10 +214,12 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
             if (!ok) break;                        // stop consuming and issuing; abort below
             if (tg.x & 1) {
                 if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
-                else accumulate_records(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
+                else if (kBatch) accumulate_records<2>(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
+                else accumulate_records_1(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
             } else {
                 if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
-                else accumulate_records(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
+                else if (kBatch) accumulate_records<2>(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
+                else accumulate_records_1(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
             }
             consumed++;
             __syncwarp();
@@ -308,10 +315,10 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
     cluster_sync();                            // no CTA leaves while a remote store may target it
 }
 
-template <int VARIANT>
+template <int VARIANT, bool kBatch>
 static cudaError_t launch_one(const SweepParams& p, int n_units, size_t smem, cudaStream_t st, bool check_only,
                               int* max_clusters) {
-    auto kern = sweep_cluster_kernel<VARIANT>;
+    auto kern = sweep_cluster_kernel<VARIANT, kBatch>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess && p.cluster > 8) e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
@@ -341,8 +348,16 @@ cudaError_t launch_sweep_cluster(const SweepParams& p, int n_units, int variant,
     if (p.cluster < 2 || p.cluster > 16 || (kSplit % (p.cluster * p.warps)) != 0) return cudaErrorInvalidValue;
     const size_t smem = cluster_smem_bytes(max_N, p.warps, p.cluster);
     const bool check = max_clusters != nullptr;
-    return variant == 0 ? launch_one<0>(p, n_units, smem, st, check, max_clusters)
-                        : launch_one<1>(p, n_units, smem, st, check, max_clusters);
+    int sms = 0, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms = 148;
+    // batched record loads when the launch leaves SMs without a CTA
+    const bool batch = (long long)n_units * p.cluster <= sms;
+    if (variant == 0)
+        return batch ? launch_one<0, true>(p, n_units, smem, st, check, max_clusters)
+                     : launch_one<0, false>(p, n_units, smem, st, check, max_clusters);
+    return batch ? launch_one<1, true>(p, n_units, smem, st, check, max_clusters)
+                 : launch_one<1, false>(p, n_units, smem, st, check, max_clusters);
 }
 
 size_t cluster_smem_bytes_host(int N, int warps, int C) { return cluster_smem_bytes(N, warps, C); }

@@ -289,9 +289,11 @@ __device__ __forceinline__ void accumulate_chunk(const int2* __restrict__ R, int
 // The same groups stored as 16-byte records {g, o2, p<<16|o1, last}, one
 // per data entry: a record's position does not depend on an earlier header.
 // Records are taken kUnroll at a time with their shared-memory loads (the
-// records, then each a_o2, and a_p, a_o1 where the record ends a group --
-// predicated, so no other record reads them) issued before the arithmetic,
-// so a batch costs about two load latencies.  The arithmetic is
+// records, then each record's a_o2, a_p, a_o1, the last two used only where
+// the record ends a group) issued before the arithmetic, so a batch costs
+// about two load latencies: for chains that wait on latency (a few warps
+// per SM).  Kernels that fill the SMs use accumulate_records_k's one record
+// at a time, which loads a_p, a_o1 once per group.  The arithmetic is
 // accumulate_chunk's, operation for operation: Y accumulates the group's
 // entries in order from zero and h takes a_p conj(a_o1) Y at the group's
 // last record.  kSingle: every record ends its group (groups of one entry,
@@ -328,11 +330,8 @@ __device__ __forceinline__ void accumulate_records(const int2* __restrict__ R2, 
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) {
             a[u] = sp[q[u].y * kRepBlock + lane];
-            ap[u] = ao[u] = make_float2(0.f, 0.f);
-            if (kSingle || q[u].w) {
-                ap[u] = sp[(q[u].z >> 16) * kRepBlock + lane];
-                ao[u] = sp[(q[u].z & 0xFFFF) * kRepBlock + lane];
-            }
+            ap[u] = sp[(q[u].z >> 16) * kRepBlock + lane];
+            ao[u] = sp[(q[u].z & 0xFFFF) * kRepBlock + lane];
         }
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) record_step<kSingle>(q[u], a[u], ap[u], ao[u], yx, yy, hx, hy);
@@ -441,6 +440,10 @@ __device__ __forceinline__ void accumulate_tiles_k(const int2* __restrict__ R2, 
     }
 }
 
+// One record at a time (accumulate_records_k for one replica per lane).
+__device__ __forceinline__ void accumulate_records_1(const int2* __restrict__ R2, int n,
+                                                     const float2* __restrict__ sp, int lane, float& hx, float& hy);
+
 template <int K>
 __device__ __forceinline__ void accumulate_records_k(const int2* __restrict__ R2, int n,
                                                      const float2* __restrict__ sp, int lane,
@@ -450,37 +453,39 @@ __device__ __forceinline__ void accumulate_records_k(const int2* __restrict__ R2
     float yx[K], yy[K];
 #pragma unroll
     for (int k = 0; k < K; k++) yx[k] = yy[k] = 0.f;
-    constexpr int kB = 2;                // records per batch (K amplitudes each)
-    int r = 0;
-    for (; r + kB <= nr; r += kB) {
-        int4 q[kB];
-        float2 a[kB][K], ap[kB][K], ao[kB][K];
+#pragma unroll 4
+    for (int r = 0; r < nr; r++) {
+        const int4 q = R[r];
+        const float g = __int_as_float(q.x);
 #pragma unroll
-        for (int u = 0; u < kB; u++) q[u] = R[r + u];
-#pragma unroll
-        for (int u = 0; u < kB; u++)
+        for (int k = 0; k < K; k++) {
+            const float2 a = sp[(q.y * K + k) * kRepBlock + lane];
+            yx[k] = fmaf(g, a.x, yx[k]);
+            yy[k] = fmaf(-g, a.y, yy[k]);
+        }
+        if (q.w) {
+            const int p = q.z >> 16, o1 = q.z & 0xFFFF;
 #pragma unroll
             for (int k = 0; k < K; k++) {
-                a[u][k] = sp[(q[u].y * K + k) * kRepBlock + lane];
-                ap[u][k] = ao[u][k] = make_float2(0.f, 0.f);
-                if (q[u].w) {
-                    ap[u][k] = sp[((q[u].z >> 16) * K + k) * kRepBlock + lane];
-                    ao[u][k] = sp[((q[u].z & 0xFFFF) * K + k) * kRepBlock + lane];
-                }
+                const float2 ap = sp[(p * K + k) * kRepBlock + lane];
+                const float2 ao = sp[(o1 * K + k) * kRepBlock + lane];
+                const float px = fmaf(ap.x, ao.x, ap.y * ao.y);
+                const float py = fmaf(ap.y, ao.x, -ap.x * ao.y);
+                hx[k] = fmaf(px, yx[k], fmaf(-py, yy[k], hx[k]));
+                hy[k] = fmaf(px, yy[k], fmaf(py, yx[k], hy[k]));
+                yx[k] = 0.f;
+                yy[k] = 0.f;
             }
-#pragma unroll
-        for (int u = 0; u < kB; u++)
-#pragma unroll
-            for (int k = 0; k < K; k++)
-                record_step<false>(q[u], a[u][k], ap[u][k], ao[u][k], yx[k], yy[k], hx[k], hy[k]);
+        }
     }
-    for (; r < nr; r++) {
-        const int4 q = R[r];
-#pragma unroll
-        for (int k = 0; k < K; k++)
-            record_step<false>(q, sp[(q.y * K + k) * kRepBlock + lane], sp[((q.z >> 16) * K + k) * kRepBlock + lane],
-                               sp[((q.z & 0xFFFF) * K + k) * kRepBlock + lane], yx[k], yy[k], hx[k], hy[k]);
-    }
+}
+
+__device__ __forceinline__ void accumulate_records_1(const int2* __restrict__ R2, int n,
+                                                     const float2* __restrict__ sp, int lane, float& hx, float& hy) {
+    float hx1[1] = {hx}, hy1[1] = {hy};
+    accumulate_records_k<1>(R2, n, sp, lane, hx1, hy1);
+    hx = hx1[0];
+    hy = hy1[0];
 }
 
 // The field partials of the C CTAs x W warps of a block, summed in the fixed
