@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
                 if (which >= 2) accumulate_chunk(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
                 else if (S.fc_tiles)               // unrolled by 2: the kernel is held to 80 registers
                     accumulate_tiles<2>(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
-                else accumulate_records<2>(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
+                else accumulate_records_1(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
                 consumed++;
                 __syncwarp();
                 if (lane == 0) fence_async_shared();

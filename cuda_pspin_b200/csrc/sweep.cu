@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(256, 3) sweep_kernel(const SweepParams P) {
                 if (!ok) break;                    // stop consuming and issuing; abort below
                 const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
                 if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
-                else accumulate_records<2>(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
+                else accumulate_records_1(ring + slot * kStage, n, sp, lane, h[2 * which], h[2 * which + 1]);
                 consumed++;
                 __syncwarp();
                 if (lane == 0) fence_async_shared();
