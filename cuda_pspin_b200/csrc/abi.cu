@@ -172,6 +172,7 @@ struct pspin_state {
     int64_t* d_chunk_start = nullptr;
     int* d_site_chunks = nullptr;
     int* d_pair_chunks = nullptr;       // pair sub-lists, built on the first two-pass proposal
+    int* d_site_chunks_g = nullptr;     // site lists in the group format, built with the pair sub-lists
     uint32_t* d_nbmask = nullptr;       // per sample: neighbour masks (rows of ceil(N/32) words)
     int64_t ent_total = 0, chunk_total = 0;
     Q64* d_q64 = nullptr;
@@ -247,7 +248,7 @@ static void free_state(pspin_state* s) {
                     s->d_beta_sched, s->d_perm, s->d_drand, s->d_ex_acc, s->d_ex_prop, s->d_trace,
                     s->d_tc_w, s->d_tc_x, s->d_tc_f, s->d_tc_ws, s->d_tc_h, s->d_f64_h, s->d_tc_e,
                     s->d_w32, s->d_adam_m, s->d_adam_v, s->d_grad, s->d_wbf, s->d_records, s->d_rec_count,
-                    s->d_save, s->d_loss, s->d_idx, s->d_obs_E, s->d_obs_q, s->d_pair_chunks, s->d_nbmask,
+                    s->d_save, s->d_loss, s->d_idx, s->d_obs_E, s->d_obs_q, s->d_pair_chunks, s->d_site_chunks_g, s->d_nbmask,
                     s->d_units_k[0], s->d_units_k[1]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1115,6 +1116,7 @@ static int enqueue_step(pspin_state* s, int nsweeps, bool exchange, cudaEvent_t 
     p.chunk_start = s->d_chunk_start;
     p.site_chunks = s->d_site_chunks;
     p.pair_chunks = s->d_pair_chunks;
+    p.site_chunks_g = s->d_site_chunks_g;
     p.nbmask = s->d_nbmask;
     p.sweep_counter = s->d_sweep_counter;
     p.nsweeps = nsweeps;
@@ -1140,6 +1142,8 @@ static int enqueue_step(pspin_state* s, int nsweeps, bool exchange, cudaEvent_t 
     } else if (s->proposal == PSPIN_PROPOSAL_PLAIN) {
         CK(launch_sweep(p, (int)s->units.size(), s->variant, s->max_N, s->st));
     } else {
+        if (!s->d_site_chunks_g || !s->d_pair_chunks)
+            return fail(PSPIN_ERR_STATE, "two-pass sweep without its group-format lists (pspin_set_proposal builds them)");
         LearnParams lp{};
         lp.mode = s->proposal;
         lp.w = s->d_wbf;
@@ -2014,7 +2018,11 @@ extern "C" int pspin_local_fields(pspin_state* s, int sample, int method, double
 // ------------------------------------------------------------------ learned proposal
 // Pair sub-lists for the two-pass sweep: rebuilt from the FP64 quartet table
 // (same couplings, rounded to FP32 like the site lists) and appended to the
-// entry and chunk arrays; d_pair_chunks indexes them per sample.
+// entry and chunk arrays; d_pair_chunks indexes them per sample.  The site
+// lists of samples without tiles are appended as well in the group format
+// (header + entries: the same groups and arithmetic as the records), which
+// the two-pass kernel reads faster; d_site_chunks_g indexes them like
+// d_site_chunks (tile samples keep their tiles).
 static int ensure_pair_lists(pspin_state* s) {
     if (s->d_pair_chunks) return PSPIN_OK;
     const int n = s->S;
@@ -2026,7 +2034,7 @@ static int ensure_pair_lists(pspin_state* s) {
                                cudaMemcpyDeviceToHost, s->st));
     }
     CK(cudaStreamSynchronize(s->st));
-    std::vector<SiteLists> pl(n);
+    std::vector<SiteLists> pl(n), gl(n);
 #pragma omp parallel for schedule(dynamic, 1)
     for (int k = 0; k < n; k++) {
         std::vector<QuartetRec> recs(q[k].size());
@@ -2036,13 +2044,19 @@ static int ensure_pair_lists(pspin_state* s) {
         }
         std::vector<Q64>().swap(q[k]);
         build_pair_lists(s->hs[k].N, s->hs[k].g2re.data(), s->hs[k].h2_active, recs, pl[k]);
+        if (!s->hs[k].fc_tiles) build_site_lists(s->hs[k].N, s->hs[k].g2re.data(), s->hs[k].h2_active, recs, gl[k], false);
     }
-    int64_t ent_new = 0, chunk_new = 0, idx_total = 0;
+    int64_t ent_new = 0, chunk_new = 0, idx_total = 0, split_total = 0;
     for (int k = 0; k < n; k++) {
-        ent_new += (int64_t)pl[k].entries.size();
-        chunk_new += (int64_t)pl[k].chunk_start.size();
+        ent_new += (int64_t)pl[k].entries.size() + (int64_t)gl[k].entries.size();
+        chunk_new += (int64_t)pl[k].chunk_start.size() + (int64_t)gl[k].chunk_start.size();
         idx_total += (int64_t)pl[k].site_chunks.size();
+        split_total += (int64_t)s->hs[k].N * (kSplit + 1);
     }
+    std::vector<int> scg((size_t)split_total);     // group-format site chunk table, tile samples as they are
+    if (split_total)
+        CK(cudaMemcpyAsync(scg.data(), s->d_site_chunks, scg.size() * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
     if (s->chunk_total + chunk_new >= (1ll << 31)) return fail(PSPIN_ERR_ARG, "too many list chunks for the pair sub-lists");
     std::vector<int2> ent((size_t)ent_new);
     std::vector<int64_t> cs((size_t)chunk_new + 1);
@@ -2059,15 +2073,26 @@ static int ensure_pair_lists(pspin_state* s) {
         coff += (int64_t)pl[k].chunk_start.size();
         ioff += (int64_t)pl[k].site_chunks.size();
         pl[k] = SiteLists();
+        if (!gl[k].entries.empty()) {
+            std::copy(gl[k].entries.begin(), gl[k].entries.end(), ent.begin() + eoff);
+            for (size_t t = 0; t < gl[k].chunk_start.size(); t++) cs[coff + t] = gl[k].chunk_start[t] + eoff + s->ent_total;
+            for (size_t t = 0; t < gl[k].site_chunks.size(); t++)
+                scg[s->sd[k].split_off + t] = (int)(gl[k].site_chunks[t] + coff + s->chunk_total);
+            eoff += (int64_t)gl[k].entries.size();
+            coff += (int64_t)gl[k].chunk_start.size();
+        }
+        gl[k] = SiteLists();
     }
     cs[chunk_new] = s->ent_total + ent_new;
     int2* d_ent = nullptr;
     int64_t* d_cs = nullptr;
     int* d_pc = nullptr;
+    int* d_scg = nullptr;
     int rc;
     if ((rc = dalloc(&d_ent, (size_t)(s->ent_total + ent_new))) ||
-        (rc = dalloc(&d_cs, (size_t)(s->chunk_total + chunk_new + 1))) || (rc = dalloc(&d_pc, (size_t)idx_total))) {
-        cudaFree(d_ent); cudaFree(d_cs); cudaFree(d_pc);
+        (rc = dalloc(&d_cs, (size_t)(s->chunk_total + chunk_new + 1))) || (rc = dalloc(&d_pc, (size_t)idx_total)) ||
+        (rc = dalloc(&d_scg, (size_t)std::max<int64_t>(split_total, 1)))) {
+        cudaFree(d_ent); cudaFree(d_cs); cudaFree(d_pc); cudaFree(d_scg);
         return rc;
     }
     std::vector<SampleDev> sd = s->sd;
@@ -2081,11 +2106,13 @@ static int ensure_pair_lists(pspin_state* s) {
         e = cudaMemcpyAsync(d_cs + s->chunk_total, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s->st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_pc, pc.data(), pc.size() * sizeof(int), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess && split_total)
+        e = cudaMemcpyAsync(d_scg, scg.data(), scg.size() * sizeof(int), cudaMemcpyHostToDevice, s->st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->d_samples, sd.data(), sd.size() * sizeof(SampleDev), cudaMemcpyHostToDevice, s->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
     if (e != cudaSuccess) {
-        cudaFree(d_ent); cudaFree(d_cs); cudaFree(d_pc);
+        cudaFree(d_ent); cudaFree(d_cs); cudaFree(d_pc); cudaFree(d_scg);
         return fail(PSPIN_ERR_CUDA, "pair sub-list upload: %s", cudaGetErrorString(e));
     }
     s->sd = sd;
@@ -2094,6 +2121,7 @@ static int ensure_pair_lists(pspin_state* s) {
     s->d_entries = d_ent;
     s->d_chunk_start = d_cs;
     s->d_pair_chunks = d_pc;
+    s->d_site_chunks_g = d_scg;
     s->ent_total += ent_new;
     s->chunk_total += chunk_new;
     return PSPIN_OK;

@@ -110,6 +110,8 @@ struct SweepParams {
     const int64_t* chunk_start;
     const int* site_chunks;
     const int* pair_chunks;           // pair sub-lists (two-pass proposals), or null
+    const int* site_chunks_g;         // the site lists in the group format (two-pass proposals;
+                                      // tiles unchanged), same per-sample offsets as site_chunks
     const uint32_t* nbmask;           // per sample: row m = sites sharing a quartet (or a g2 term) with m
     const long long* sweep_counter;   // global sweep index at launch start
     int nsweeps;

@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
     st.key0 = S.pair_key0;
     st.key1 = S.pair_key1;
     st.N = N;
-    st.site_chunks = P.site_chunks + S.split_off;
+    st.site_chunks = P.site_chunks_g + S.split_off;   // built with the pair sub-lists (set_proposal)
     st.pair_chunks = P.pair_chunks + S.pair_off;
     st.sweep0 = sweep0;
     st.steps = steps;
@@ -266,8 +266,9 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
     uint32_t xchg = 0;                         // exchanges so far (buffer parity)
     bool aborted = false;                      // set uniformly over the CTA (cluster) by reduce()
 
-    // one pass over this warp's share of two lists: the sites' lists (base 0)
-    // or the pair's sub-lists (base 2, always in the group format)
+    // one pass over this warp's share of two lists: the sites' lists (base 0;
+    // tiles, or the group format built with the pair sub-lists) or the pair's
+    // sub-lists (base 2, group format)
     auto pass = [&](int m, int base, float* h) {
         for (int which = base; which < base + 2 && ok_wait; which++) {
             int c, c_end;
@@ -278,10 +279,9 @@ __global__ void __launch_bounds__(256, 3) learned_sweep_kernel(const SweepParams
                 if (!ok_wait) break;               // stop consuming and issuing; abort in reduce()
                 const int n = (int)(__ldg(P.chunk_start + c + 1) - __ldg(P.chunk_start + c));
                 const int k2 = 2 * (which & 1);
-                if (which >= 2) accumulate_chunk(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
-                else if (S.fc_tiles)               // unrolled by 2: the kernel is held to 80 registers
+                if (which < 2 && S.fc_tiles)      // unrolled by 2: the kernel is held to 80 registers
                     accumulate_tiles<2>(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
-                else accumulate_records_1(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
+                else accumulate_chunk(ring + slot * kStage, n, sp, lane, h[k2], h[k2 + 1]);
                 consumed++;
                 __syncwarp();
                 if (lane == 0) fence_async_shared();
