@@ -57,11 +57,11 @@ inline size_t cluster_smem_bytes(int N, int warps, int C) {
 
 // kBatch: the group records are read in batches whose loads are all in
 // flight before their arithmetic (few blocks, so each warp waits on its own
-// chain's latency); otherwise one record at a time, loading a_p, a_o1 once
-// per group (many blocks share the SMs; fewer shared-memory loads and no
-// register spill at 128 registers).
+// chain's latency, and a CTA may take every register of an SM); otherwise
+// one record at a time, loading a_p, a_o1 once per group (many blocks share
+// the SMs at two CTAs each: fewer shared-memory loads, 128 registers).
 template <int VARIANT, bool kBatch>
-__global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams P) {
+__global__ void __launch_bounds__(256, kBatch ? 1 : 2) sweep_cluster_kernel(const SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int C = P.cluster;
     const uint32_t rank = cluster_rank();
@@ -214,11 +214,11 @@ __global__ void __launch_bounds__(256, 2) sweep_cluster_kernel(const SweepParams
             if (!ok) break;                        // stop consuming and issuing; abort below
             if (tg.x & 1) {
                 if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
-                else if (kBatch) accumulate_records<2>(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
+                else if (kBatch) accumulate_records<4>(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
                 else accumulate_records_1(ring + slot * kStage, tg.y, sp, lane, h[2], h[3]);
             } else {
                 if (S.fc_tiles) accumulate_tiles(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
-                else if (kBatch) accumulate_records<2>(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
+                else if (kBatch) accumulate_records<4>(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
                 else accumulate_records_1(ring + slot * kStage, tg.y, sp, lane, h[0], h[1]);
             }
             consumed++;
