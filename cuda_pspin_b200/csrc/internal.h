@@ -85,10 +85,10 @@ struct SampleDev {
     uint32_t pair_key0, pair_key1;
 };
 
-struct Unit {              // one CTA of the sweep kernel
+struct Unit {              // one replica block: a CTA, or a cluster of CTAs
     int sample;
     int rep_begin;
-    int rep_count;         // <= 32
+    int rep_count;         // <= 32 (32K with K replicas per lane)
     int pad;
 };
 
